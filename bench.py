@@ -1,0 +1,312 @@
+"""Throughput of the ERI engine on the 8-atom, 120-function workload (FP64 form).
+
+One step = one full-tensor call: the 120^4 float64 ERI tensor (1.66 GB) of the ``medium8``
+synthetic basis (8 atoms in a 10-bohr box; per atom s(6), s(3), s(1), p(3), p(1), d(1);
+Cartesian; physicist notation as a view of the chemist array, as gbasis returns it).
+
+* ``value``: unique contracted ERIs per second with the basis resident in HBM (device time of
+  K steps with CUDA events, max over ranks).
+* ``e2e``: the same metric through the public API ``electron_repulsion_integral`` with host
+  buffers: basis packing + upload (H2D) and the full tensor copied back to page-locked host
+  memory (D2H) inside every step.
+* ``roofline``: the dominant kernel phase against its bound (class kernels: FP64 FMA pipe,
+  peak measured live by ``gbx_fp64_peak``; expansion: HBM, peak from MEASURED_PEAKS.json).
+* ``cpu_baseline``: the CPU oracle (a NumPy restatement of gbasis's algorithm) on a seeded
+  sample of the workload's shell quartets, extrapolated to the whole workload.
+
+``--impl reference`` times that CPU implementation on all host cores instead and prints
+the same metric with ``"impl": "reference"``.  For N > 1 GPUs every rank computes the
+same workload (replicas; the north-star path runs on one GPU) and ``value`` aggregates.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "medium8"
+METRIC = "unique contracted ERIs/s (FP64 full tensor)"
+UNIT = "ERI/s"
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(shells, seconds=12.0, seed=0):
+    """Oracle on a seeded random sample of unique shell quartets, extrapolated."""
+    import itertools
+    from oracle import eri_oracle as orc
+    pairs = list(itertools.combinations_with_replacement(range(len(shells)), 2))
+    npair = len(pairs)
+    nq = npair * (npair + 1) // 2
+    rng = np.random.default_rng(seed)
+    t0 = time.perf_counter()
+    done = 0
+    while time.perf_counter() - t0 < seconds:
+        p, q = sorted(rng.integers(0, npair, size=2))
+        (i, j), (k, l) = pairs[p], pairs[q]
+        orc.construct_array_contraction(shells[i], shells[j], shells[k], shells[l])
+        done += 1
+    dt = time.perf_counter() - t0
+    n = sum(len(s.angmom_components_cart) for s in shells)
+    from gbasis_b200.flops import unique_eris
+    est_total = dt / done * nq
+    return {"value": unique_eris(n) / est_total, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{done} random unique shell quartets of {nq} ({dt:.1f} s, "
+                      f"oracle construct_array_contraction, 1 core), extrapolated"}
+
+
+def _pool_worker(args):
+    import itertools
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from gbasis_b200.synthetic import make_workload
+    from oracle import eri_oracle as orc
+    seed, seconds = args
+    shells = make_workload(WORKLOAD)
+    pairs = list(itertools.combinations_with_replacement(range(len(shells)), 2))
+    rng = np.random.default_rng(seed)
+    t0 = time.perf_counter()
+    done = 0
+    while time.perf_counter() - t0 < seconds:
+        p, q = sorted(rng.integers(0, len(pairs), size=2))
+        (i, j), (k, l) = pairs[p], pairs[q]
+        orc.construct_array_contraction(shells[i], shells[j], shells[k], shells[l])
+        done += 1
+    return done, time.perf_counter() - t0
+
+
+def run_reference(a, rank, world):
+    """CPU implementation of the path (the oracle port) on all host cores."""
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from gbasis_b200.synthetic import make_workload
+    from gbasis_b200.flops import unique_eris
+    shells = make_workload(WORKLOAD)
+    n = sum(len(s.angmom_components_cart) for s in shells)
+    npair = len(shells) * (len(shells) + 1) // 2
+    nq = npair * (npair + 1) // 2
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    per_step = 4.0
+    vals = []
+    with ctx.Pool(cores) as pool:
+        for step in range(a.warmup + a.steps):
+            res = pool.map(_pool_worker, [(1000 * step + r, per_step) for r in range(cores)])
+            done = sum(d for d, _ in res)
+            wall = max(t for _, t in res)
+            rate_q = done / wall  # quartets per second, all cores
+            v = unique_eris(n) / (nq / rate_q)
+            if step >= a.warmup:
+                vals.append(v)
+    v = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": unique_eris(n) / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_functions": n, "shell_quartets": nq,
+                       "notation": "physicist", "coord_type": "cartesian"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{per_step:.0f} s per step per core of random unique "
+                                       f"shell quartets, extrapolated to {nq} quartets"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    a = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return run_reference(a, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from gbasis_b200 import _engine
+    from gbasis_b200 import electron_repulsion as er
+    from gbasis_b200.flops import basis_flops, unique_eris
+    from gbasis_b200.synthetic import make_workload
+
+    shells = make_workload(WORKLOAD)
+    n = sum(len(s.angmom_components_cart) for s in shells)
+    n_unique = unique_eris(n)
+    flops = basis_flops(shells)
+    dev = torch.device("cuda", local)
+    db = _engine.DeviceBasis(shells, device=local)
+    nq, compact_bytes = db.stats()
+    out = torch.empty(n ** 4, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = __import__("ctypes").c_void_p(stream.cuda_stream)
+
+    def step():
+        db.full_device(out.data_ptr(), "chemist", 0.0, stream=sp)
+
+    for _ in range(max(3, a.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(a.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n_unique / (ms * 1e-3)
+
+    # per-phase device times (events on the same stream), a separate pass of the same call
+    db.set_profiling(True)
+    ph = np.zeros(3)
+    for _ in range(a.steps):
+        step()
+        ph += db.phase_times()
+    ph /= a.steps
+    db.set_profiling(False)
+    peak64 = _engine.fp64_peak(local)
+    peaks = _peaks()
+    hbm = peaks.get("hbm_gbs")
+    compute_tf = flops / (ph[1] * 1e-3) / 1e12
+    exp_bytes = 8.0 * n ** 4 + compact_bytes  # tensor written + compact store read once
+    exp_gbs = exp_bytes / (ph[2] * 1e-3) / 1e9
+    roof_compute = {"kernel": "eri_block_fp64 (all classes)", "bound": "fp64", "achieved": compute_tf,
+                    "peak": peak64, "unit": "TFLOP/s", "frac": compute_tf / peak64,
+                    "peak_source": "gbx_fp64_peak dependent-FMA probe, measured live",
+                    "traffic": None, "ms": ph[1], "algorithmic_flops": flops}
+    roof_expand = {"kernel": "expand_full", "bound": "hbm", "achieved": exp_gbs, "peak": hbm,
+                   "unit": "GB/s", "frac": (exp_gbs / hbm) if hbm else None,
+                   "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                   "traffic": None, "ms": ph[2], "algorithmic_bytes": exp_bytes}
+    roof = roof_compute if ph[1] >= ph[2] else roof_expand
+
+    # end to end through the public API with host buffers
+    pinned = torch.empty(n ** 4, dtype=torch.float64, pin_memory=True).numpy().reshape((n,) * 4)
+    pk = _engine.pack_basis(shells)
+    h2d = sum(int(v.nbytes) for v in pk.values())
+    er.electron_repulsion_integral(shells, out=pinned)  # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.e2e_steps):
+        res = er.electron_repulsion_integral(shells, out=pinned)
+    e2e_s = (time.perf_counter() - t0) / a.e2e_steps
+    assert res.shape == (n, n, n, n)
+    e2e = {"value": world * n_unique / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": 8 * n ** 4, "ms_per_step": e2e_s * 1e3}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_functions": n, "shell_quartets": nq,
+                       "unique_eris": n_unique, "notation": "physicist", "coord_type": "cartesian",
+                       "form": "fp64", "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "working set above L2 (1.66 GB tensor, "
+                             f"{compact_bytes / 1e6:.0f} MB compact store)"},
+            "phases_ms": {"work_list": ph[0], "class_kernels": ph[1], "expand": ph[2]},
+            "roofline": roof, "roofline_kernels": [roof_compute, roof_expand],
+            "e2e": e2e, "clocks": clk.summary(),
+            "gpu_launches": None}
+    # our kernels per step: work-list build + one per class block + expansion
+    import gbasis_b200._engine as eng  # noqa: F401
+    line["gpu_launches"] = a.steps * (2 + _num_blocks(shells))
+    if rank == 0 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(shells)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    db.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _num_blocks(shells):
+    ls = set()
+    for s in shells:
+        ls.add(s.angmom)
+    pcs = sorted({(max(a, b), min(a, b)) for a in ls for b in ls})
+    return len(pcs) * (len(pcs) + 1) // 2
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,301 @@
+"""ctypes binding of ``libgbx_eri.so`` (the C ABI declared in ``include/gbx_eri.h``).
+
+The library is built in-tree by ``python -m gbasis_b200.build``.  Loading fails loudly when
+it is missing or when no CUDA device is present: the engine has no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+from .contractions import is_shell
+
+__all__ = ["lib", "EngineError", "check", "pack_basis", "DeviceBasis", "EXPORTED_SYMBOLS",
+           "library_path", "fp64_peak"]
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libgbx_eri.so")
+
+GBX_OK, GBX_ERR_INVALID, GBX_ERR_UNSUPPORTED, GBX_ERR_OOM, GBX_ERR_CUDA, GBX_ERR_TIMEOUT = range(6)
+GBX_CHEMIST, GBX_PHYSICIST = 0, 1
+MAX_CART = 10
+
+EXPORTED_SYMBOLS = (
+    "gbx_basis_create", "gbx_basis_destroy", "gbx_basis_nbf", "gbx_basis_stats",
+    "gbx_basis_set_groups", "gbx_eri_full", "gbx_eri_full_host", "gbx_schwarz_bounds",
+    "gbx_lincomb", "gbx_eri_coulomb_j", "gbx_last_counts", "gbx_last_error", "gbx_fp64_peak",
+    "gbx_set_profiling", "gbx_phase_times",
+)
+
+
+class EngineError(RuntimeError):
+    """A CUDA-side failure of the engine (launch error, device fault, timeout)."""
+
+
+_lib = None
+_lock = threading.Lock()
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_I64 = ctypes.c_int64
+
+
+def library_path():
+    return LIB_PATH
+
+
+def lib():
+    """Load the engine library (once)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is not built; run `python -m gbasis_b200.build` (needs nvcc)")
+        L = ctypes.CDLL(LIB_PATH)
+        sig = {
+            "gbx_basis_create": [ctypes.POINTER(_P), _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I],
+            "gbx_basis_destroy": [_P],
+            "gbx_basis_nbf": [_P, ctypes.POINTER(_I64)],
+            "gbx_basis_stats": [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
+            "gbx_basis_set_groups": [_P, _P],
+            "gbx_eri_full": [_P, _I, _D, _P, _P],
+            "gbx_eri_full_host": [_P, _I, _D, _P, _P],
+            "gbx_schwarz_bounds": [_P, _P],
+            "gbx_lincomb": [_P, _I64, _P, _I64, _P, _P, _P],
+            "gbx_eri_coulomb_j": [_P, _P, _D, _P, _P],
+            "gbx_last_counts": [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
+            "gbx_last_error": [ctypes.c_char_p, ctypes.c_size_t],
+            "gbx_fp64_peak": [_I, ctypes.POINTER(_D)],
+            "gbx_set_profiling": [_P, _I],
+            "gbx_phase_times": [_P, _P],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = _I
+        _lib = L
+        return L
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(2048)
+    lib().gbx_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(code, what=""):
+    """Map a C-ABI status code to a Python exception."""
+    if code == GBX_OK:
+        return
+    msg = f"{what}: {last_error()}" if what else last_error()
+    if code == GBX_ERR_INVALID:
+        raise ValueError(msg)
+    if code == GBX_ERR_UNSUPPORTED:
+        raise NotImplementedError(msg)
+    if code == GBX_ERR_OOM:
+        raise MemoryError(msg)
+    if code == GBX_ERR_TIMEOUT:
+        raise TimeoutError(msg)
+    raise EngineError(msg)
+
+
+# ---------------------------------------------------------------------------- packing
+def _dfact(n):
+    r = 1
+    while n > 1:
+        r *= n
+        n -= 2
+    return r
+
+
+def _canon_cart(l):
+    return [(x, y, l - x - y) for x in range(l, -1, -1) for y in range(l - x, -1, -1)]
+
+
+def _canon_sph_labels(l):
+    return [f"s{m}" for m in range(l, 0, -1)] + [f"c{m}" for m in range(l + 1)]
+
+
+# real solid harmonics of l <= 1 as Cartesian components: s -> 1; p: c1=x, s1=y, c0=z
+_P_LABEL = {(1, 0, 0): "c1", (0, 1, 0): "s1", (0, 0, 1): "c0"}
+
+
+def _norm_cont(shell):
+    coeffs = np.asarray(shell.coeffs)
+    M = coeffs.shape[1] if coeffs.ndim == 2 else 1
+    L = len(shell.angmom_components_cart)
+    return np.asarray(shell.norm_cont, dtype=float).reshape(M, L)
+
+
+def _coord_type(shell, override=None):
+    ct = override if override is not None else shell.coord_type
+    ct = {"c": "cartesian", "p": "spherical"}.get(ct, ct)
+    if ct not in ("cartesian", "spherical"):
+        raise ValueError("Each entry of `coord_types` must be one of 'cartesian' or 'spherical'.")
+    return ct
+
+
+def pack_basis(shells, coord_types=None, raw=False):
+    """Flatten shells into the per-segmented-contraction arrays of ``gbx_basis_create``.
+
+    ``raw=True`` packs the layout of ``construct_array_contraction``: Cartesian components in
+    each shell's order with the component norm, without ``norm_cont``.
+    Returns a dict of numpy arrays plus the segment -> (shell, m) map.
+    """
+    ang, npr, cen, exps, coefs, nout, sph, pos, scl, group = ([] for _ in range(10))
+    for si, sh in enumerate(shells):
+        if not is_shell(sh):
+            raise TypeError("Given contractions must be instances of the "
+                            "`GeneralizedContractionShell` class.")
+        l = int(sh.angmom)
+        e = np.asarray(sh.exps, dtype=float).ravel()
+        c = np.asarray(sh.coeffs, dtype=float)
+        c = c[:, None] if c.ndim == 1 else c
+        ct = "cartesian" if raw else _coord_type(sh, None if coord_types is None else coord_types[si])
+        cart = [tuple(int(v) for v in r) for r in np.asarray(sh.angmom_components_cart)]
+        if sorted(cart) != sorted(_canon_cart(l)):
+            raise ValueError(f"shell {si}: angmom_components_cart is not a permutation of the "
+                             f"{len(_canon_cart(l))} components of l={l}")
+        nc = np.ones((c.shape[1], len(cart))) if raw else _norm_cont(sh)
+        for m in range(c.shape[1]):
+            p = np.full(MAX_CART, -1, dtype=np.int8)
+            s = np.zeros(MAX_CART)
+            if ct == "cartesian":
+                for k, comp in enumerate(_canon_cart(l)):
+                    j = cart.index(comp)
+                    p[k] = j
+                    s[k] = nc[m, j] / np.sqrt(_dfact(2 * comp[0] - 1) * _dfact(2 * comp[1] - 1)
+                                               * _dfact(2 * comp[2] - 1))
+                n_o = len(cart)
+            else:
+                if not np.allclose(nc[m], nc[m][0], rtol=1e-14, atol=0):
+                    raise NotImplementedError(
+                        f"shell {si}: spherical transform with component-dependent norm_cont")
+                labels = list(sh.angmom_components_sph)
+                bare = [lab.lstrip("-") for lab in labels]
+                if l >= 2:
+                    internal = _canon_sph_labels(l)
+                    coef = [1.0] * len(internal)
+                else:
+                    internal = ["c0"] if l == 0 else [_P_LABEL[cc] for cc in _canon_cart(1)]
+                    coef = [1.0] * len(internal)
+                for k, lab in enumerate(internal):
+                    j = bare.index(lab)
+                    p[k] = j
+                    s[k] = nc[m][0] * coef[k] * (-1.0 if labels[j].startswith("-") else 1.0)
+                n_o = 2 * l + 1
+            ang.append(l)
+            npr.append(len(e))
+            cen.extend(np.asarray(sh.coord, dtype=float).ravel().tolist())
+            exps.extend(e.tolist())
+            coefs.extend(c[:, m].tolist())
+            nout.append(n_o)
+            sph.append(1 if ct == "spherical" else 0)
+            pos.append(p)
+            scl.append(s)
+            group.append(si)
+    return {
+        "angmom": np.array(ang, dtype=np.int32), "nprim": np.array(npr, dtype=np.int32),
+        "center": np.array(cen, dtype=np.float64), "exps": np.array(exps, dtype=np.float64),
+        "coefs": np.array(coefs, dtype=np.float64), "nout": np.array(nout, dtype=np.int32),
+        "sph": np.array(sph, dtype=np.int32), "pos": np.array(pos, dtype=np.int8).ravel(),
+        "scl": np.array(scl, dtype=np.float64).ravel(), "group": np.array(group, dtype=np.int32),
+    }
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class DeviceBasis:
+    """A basis resident on one CUDA device (owns a ``gbx_basis`` handle)."""
+
+    def __init__(self, shells, coord_types=None, raw=False, device=None):
+        L = lib()
+        if device is None:
+            device = _current_device()
+        self.packed = pk = pack_basis(shells, coord_types, raw)
+        h = ctypes.c_void_p()
+        check(L.gbx_basis_create(ctypes.byref(h), len(pk["angmom"]), _ptr(pk["angmom"]),
+                                 _ptr(pk["nprim"]), _ptr(pk["center"]), _ptr(pk["exps"]),
+                                 _ptr(pk["coefs"]), _ptr(pk["nout"]), _ptr(pk["sph"]),
+                                 _ptr(pk["pos"]), _ptr(pk["scl"]), int(device)),
+              "gbx_basis_create")
+        self.handle = h
+        self.device = int(device)
+        check(L.gbx_basis_set_groups(h, _ptr(pk["group"])), "gbx_basis_set_groups")
+        n = ctypes.c_int64()
+        check(L.gbx_basis_nbf(h, ctypes.byref(n)))
+        self.nbf = int(n.value)
+
+    def stats(self):
+        q, b = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().gbx_basis_stats(self.handle, ctypes.byref(q), ctypes.byref(b)))
+        return int(q.value), int(b.value)
+
+    def full_host(self, notation="chemist", schwarz_threshold=0.0, out=None, stream=None):
+        n = self.nbf
+        if out is None:
+            out = np.empty((n, n, n, n), dtype=np.float64)
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == n ** 4
+        code = GBX_PHYSICIST if notation == "physicist" else GBX_CHEMIST
+        check(lib().gbx_eri_full_host(self.handle, code, float(schwarz_threshold), _ptr(out),
+                                      stream), "gbx_eri_full_host")
+        return out
+
+    def full_device(self, out_ptr, notation="chemist", schwarz_threshold=0.0, stream=None):
+        code = GBX_PHYSICIST if notation == "physicist" else GBX_CHEMIST
+        check(lib().gbx_eri_full(self.handle, code, float(schwarz_threshold),
+                                 ctypes.c_void_p(out_ptr), stream), "gbx_eri_full")
+
+    def schwarz_bounds(self):
+        ns = len(self.packed["angmom"])
+        q = np.empty((ns, ns))
+        check(lib().gbx_schwarz_bounds(self.handle, _ptr(q)), "gbx_schwarz_bounds")
+        return q
+
+    def set_profiling(self, on=True):
+        check(lib().gbx_set_profiling(self.handle, int(bool(on))), "gbx_set_profiling")
+
+    def phase_times(self):
+        """(work-list build, class kernels, expansion) of the last call, milliseconds."""
+        ms = np.zeros(3)
+        check(lib().gbx_phase_times(self.handle, _ptr(ms)), "gbx_phase_times")
+        return ms
+
+    def last_counts(self):
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().gbx_last_counts(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return int(a.value), int(b.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().gbx_basis_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _current_device():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return torch.cuda.current_device()
+    except Exception:
+        pass
+    return 0
+
+
+def fp64_peak(device=0):
+    v = ctypes.c_double()
+    check(lib().gbx_fp64_peak(int(device), ctypes.byref(v)), "gbx_fp64_peak")
+    return float(v.value)

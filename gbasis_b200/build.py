@@ -1,0 +1,104 @@
+"""Build ``gbasis_b200/_lib/libgbx_eri.so`` for sm_100a (B200).
+
+Steps: generate the class-specialised recursion sources (``csrc/gen_eri.py``) into
+``csrc/_gen``, compile every ``.cu`` with nvcc in parallel, link one shared library.
+Run: ``python -m gbasis_b200.build [--lmax 2] [-j 8] [--force]``.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+GEN = os.path.join(CSRC, "_gen")
+BUILD = os.path.join(HERE, "_build")
+LIBDIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(LIBDIR, "libgbx_eri.so")
+LMAX_DEFAULT = 2
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
+              "-I", os.path.join(ROOT, "include"), "-I", CSRC, "-I", GEN] + ARCH
+
+
+def nvcc():
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def sources(lmax):
+    sys.path.insert(0, CSRC)
+    import gen_eri  # noqa: E402
+    gen = gen_eri.emit_sources(GEN, lmax)
+    return [os.path.join(GEN, g) for g in gen] + [
+        os.path.join(CSRC, f) for f in ("runtime.cu", "pipeline.cu", "extras.cu")]
+
+
+KERNEL_DEPS = ("gbx_common.cuh", "eri_kernels.cuh", "errors.h", "_gen/eri_gen.cuh")
+HOST_DEPS = ("gbx_common.cuh", "runtime.h", "errors.h")
+
+
+def _deps_mtime(src):
+    deps = KERNEL_DEPS if os.path.basename(src).startswith("eri_cls") else HOST_DEPS
+    m = os.path.getmtime(os.path.join(ROOT, "include", "gbx_eri.h"))
+    for d in deps:
+        p = os.path.join(CSRC, d)
+        if os.path.exists(p):
+            m = max(m, os.path.getmtime(p))
+    return m
+
+
+def compile_one(src, force, verbose_ptxas=False):
+    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(
+            os.path.getmtime(src), _deps_mtime(src)):
+        return obj, 0.0, ""
+    cmd = [nvcc(), *NVCC_FLAGS, "-c", src, "-o", obj]
+    if verbose_ptxas:
+        cmd += ["-Xptxas", "-v"]
+    t = time.time()
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr[-6000:]}")
+    return obj, time.time() - t, r.stderr
+
+
+def build(lmax=LMAX_DEFAULT, jobs=None, force=False, verbose=False, ptxas=False):
+    os.makedirs(BUILD, exist_ok=True)
+    os.makedirs(LIBDIR, exist_ok=True)
+    srcs = sources(lmax)
+    jobs = jobs or max(1, min(len(srcs), os.cpu_count() or 4))
+    objs = []
+    with cf.ThreadPoolExecutor(jobs) as ex:
+        for obj, dt, err in ex.map(lambda s: compile_one(s, force, ptxas), srcs):
+            objs.append(obj)
+            if verbose and dt:
+                print(f"  {os.path.basename(obj)}: {dt:.1f}s", flush=True)
+            if ptxas and err:
+                print(err)
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcublas", "-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--lmax", type=int, default=LMAX_DEFAULT)
+    ap.add_argument("-j", type=int, default=None)
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--ptxas", action="store_true")
+    a = ap.parse_args()
+    t = time.time()
+    print(build(a.lmax, a.j, a.force, verbose=True, ptxas=a.ptxas), f"{time.time() - t:.1f}s")

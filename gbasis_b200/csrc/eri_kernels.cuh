@@ -1,0 +1,204 @@
+// Class-templated ERI kernels (FP64 form).
+//
+// One thread owns one contracted shell quartet (bra pair p, ket pair q) of a class block:
+// it loops over the primitive quartets, evaluates F_m(T) from a shared-memory Taylor table,
+// runs the generated VRR+ETR into register accumulators [e0|f0], then the generated HRR,
+// the Cartesian->spherical transform (constant code) and the per-function permutation /
+// scale, and stores the block into the compact store.
+//
+// Reference mathematics: gbasis/integrals/_two_elec_int.py:293-812 (prefactor, VRR, ETR,
+// contraction, HRR, component norm) and gbasis/base_four_symm.py:195-349 (norm_cont,
+// spherical transform).
+#pragma once
+#include "gbx_common.cuh"
+#include "eri_gen.cuh"
+
+namespace gbx {
+
+constexpr int kEriThreads = 128;
+
+__device__ __forceinline__ constexpr double inv_odd(int m) { return 1.0 / (2 * m + 1); }
+
+// Boys function F_0..F_L(T).  T < 40: Taylor expansion of F_L around the nearest grid point
+// T_n = n/10 (8 terms, |T - T_n| <= 0.05, remainder < 1e-15 relative) from the staged table
+// g[n][k] = F_{L+k}(T_n)/k!, e^{-T} = e^{-T_n} e^{T_n - T} by the same Taylor series, then
+// the downward recursion F_m = (2T F_{m+1} + e^{-T})/(2m+1).  T >= 40: F_0 = sqrt(pi/T)/2
+// (erfc(sqrt(40)) < 1e-18) and the upward recursion F_{m+1} = ((2m+1) F_m - e^{-T})/(2T).
+// Reference: gbasis/integrals/boys_functions.py:26-63 (definition), :102-142 (recursion).
+template <int L>
+__device__ __forceinline__ void boys_eval(double T, const double* __restrict__ s_tab,
+                                          const double* __restrict__ s_exp, double* F) {
+  if (T < kBoysTMax) {
+    const int n = __double2int_rn(T * 10.0);
+    const double x = fma(-T, 10.0, (double)n) * 0.1;  // T_n - T
+    const double* g = s_tab + n * kBoysTaylor;
+    double f = g[kBoysTaylor - 1];
+#pragma unroll
+    for (int k = kBoysTaylor - 2; k >= 0; --k) f = fma(f, x, g[k]);
+    F[L] = f;
+    if (L > 0) {
+      double e = 1.0 / 5040.0;
+      e = fma(e, x, 1.0 / 720.0);
+      e = fma(e, x, 1.0 / 120.0);
+      e = fma(e, x, 1.0 / 24.0);
+      e = fma(e, x, 1.0 / 6.0);
+      e = fma(e, x, 0.5);
+      e = fma(e, x, 1.0);
+      e = fma(e, x, 1.0);
+      const double emT = s_exp[n] * e;
+      const double t2 = 2.0 * T;
+#pragma unroll
+      for (int m = L - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], emT) * inv_odd(m);
+    }
+  } else {
+    const double r = rsqrt(T);
+    F[0] = 0.88622692545275801365 * r;  // sqrt(pi)/2
+    if (L > 0) {
+      const double emT = exp(-T);
+      const double o2T = 0.5 * r * r;
+#pragma unroll
+      for (int m = 0; m < L; ++m) F[m + 1] = fma((double)(2 * m + 1), F[m], -emT) * o2T;
+    }
+  }
+}
+
+// In-place Cartesian->spherical transform of one axis of a [OUTER][ncart(L)][INNER] array.
+template <int L, int OUTER, int INNER>
+__device__ __forceinline__ void sph_axis(double* v) {
+  if constexpr (L >= 2) {
+#pragma unroll
+    for (int o = 0; o < OUTER; ++o) {
+#pragma unroll
+      for (int i = 0; i < INNER; ++i) {
+        double x[ncart(L)], y[2 * L + 1];
+#pragma unroll
+        for (int c = 0; c < ncart(L); ++c) x[c] = v[(o * ncart(L) + c) * INNER + i];
+        gen::Sph<L>::apply(x, y);
+#pragma unroll
+        for (int u = 0; u < 2 * L + 1; ++u) v[(o * ncart(L) + u) * INNER + i] = y[u];
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int internal_count(const ShellDev& s) {
+  return (s.sph && s.l >= 2) ? 2 * s.l + 1 : ncart(s.l);
+}
+
+// Stage F_{L+k}(T_n)/k! (k < kBoysTaylor) and e^{-T_n} into shared memory.
+template <int L>
+__device__ __forceinline__ void stage_boys(const double* __restrict__ tab, double* s_tab,
+                                           double* s_exp) {
+  constexpr double inv_fact[8] = {1.0, 1.0, 0.5, 1.0 / 6, 1.0 / 24, 1.0 / 120, 1.0 / 720,
+                                  1.0 / 5040};
+  for (int idx = threadIdx.x; idx < kBoysNGrid * kBoysTaylor; idx += blockDim.x) {
+    const int n = idx / kBoysTaylor, k = idx % kBoysTaylor;
+    s_tab[idx] = tab[n * (kBoysOrders + 1) + L + k] * inv_fact[k];
+  }
+  for (int n = threadIdx.x; n < kBoysNGrid; n += blockDim.x)
+    s_exp[n] = tab[n * (kBoysOrders + 1) + kBoysOrders];
+}
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(kEriThreads) eri_block_fp64(const EriLaunch a) {
+  using C = gen::Cls<LA, LB, LC, LD>;
+  constexpr int L = C::L;
+  constexpr int NCA = ncart(LA), NCB = ncart(LB), NCC = ncart(LC), NCD = ncart(LD);
+  __shared__ double s_tab[kBoysNGrid * kBoysTaylor];
+  __shared__ double s_exp[kBoysNGrid];
+  stage_boys<L>(a.boys_tab, s_tab, s_exp);
+  __syncthreads();
+
+  const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < count; w += stride) {
+    const int2 pq = a.work[a.work_off + w];
+    const PairDev P = a.pairs[pq.x];
+    const PairDev Q = a.pairs[pq.y];
+    double acc[C::NE * C::NF];
+#pragma unroll
+    for (int i = 0; i < C::NE * C::NF; ++i) acc[i] = 0.0;
+
+    for (int ip = 0; ip < P.nprim; ++ip) {
+      const PrimPair bp = a.prims[P.prim_off + ip];
+      const double o2z = 0.5 * bp.izeta;
+      for (int jq = 0; jq < Q.nprim; ++jq) {
+        const PrimPair kp = a.prims[Q.prim_off + jq];
+        const double r = rsqrt(bp.zeta + kp.zeta);
+        const double inv = r * r;
+        const double PQx = bp.Px - kp.Px, PQy = bp.Py - kp.Py, PQz = bp.Pz - kp.Pz;
+        const double rz = kp.zeta * inv;  // rho / zeta
+        const double T = bp.zeta * rz * fma(PQx, PQx, fma(PQy, PQy, PQz * PQz));
+        double F[L + 1];
+        boys_eval<L>(T, s_tab, s_exp, F);
+        const double pref = bp.C * kp.C * r;
+#pragma unroll
+        for (int m = 0; m <= L; ++m) F[m] *= pref;
+        const double ze = bp.zeta * kp.izeta;
+        const double o2e = 0.5 * kp.izeta;
+        C::template prim<double>(F, bp.Xx, bp.Xy, bp.Xz, -rz * PQx, -rz * PQy, -rz * PQz, o2z,
+                                 rz, fma(ze, bp.Xx, kp.Xx), fma(ze, bp.Xy, kp.Xy),
+                                 fma(ze, bp.Xz, kp.Xz), ze, o2e, acc);
+      }
+    }
+
+    double out[C::NAB * C::NCD];
+    C::hrr(acc, P.ABx, P.ABy, P.ABz, Q.ABx, Q.ABy, Q.ABz, out);
+
+    if (a.mode == 1) {
+      // Schwarz diagonal quartet (p, p): max |(ab|ab)| with Cartesian component norms
+      double mx = 0.0;
+#pragma unroll
+      for (int ia = 0; ia < NCA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NCB; ++ib)
+#pragma unroll
+          for (int ic = 0; ic < NCC; ++ic)
+#pragma unroll
+            for (int id = 0; id < NCD; ++id)
+              mx = fmax(mx, fabs(out[((ia * NCB + ib) * NCC + ic) * NCD + id]) *
+                                (gen::cnorm<LA>(ia) * gen::cnorm<LB>(ib) * gen::cnorm<LC>(ic) *
+                                 gen::cnorm<LD>(id)));
+      a.qout[pq.x] = sqrt(mx);
+      continue;
+    }
+
+    const ShellDev& sA = a.shells[P.shA];
+    const ShellDev& sB = a.shells[P.shB];
+    const ShellDev& sC = a.shells[Q.shA];
+    const ShellDev& sD = a.shells[Q.shB];
+    if (LD >= 2 && sD.sph) sph_axis<LD, NCA * NCB * NCC, 1>(out);
+    if (LC >= 2 && sC.sph) sph_axis<LC, NCA * NCB, NCD>(out);
+    if (LB >= 2 && sB.sph) sph_axis<LB, NCA, NCC * NCD>(out);
+    if (LA >= 2 && sA.sph) sph_axis<LA, 1, NCB * NCC * NCD>(out);
+    const int nAi = internal_count(sA), nBi = internal_count(sB);
+    const int nCi = internal_count(sC), nDi = internal_count(sD);
+    const long long nBo = sB.nout, nDo = sD.nout;
+    double* __restrict__ dst = a.out + a.base + Q.fo;
+#pragma unroll
+    for (int ia = 0; ia < NCA; ++ia) {
+      if (ia >= nAi) break;
+      const double fa = sA.scl[ia];
+      const long long ra = (long long)P.fo + sA.pos[ia] * nBo;
+#pragma unroll
+      for (int ib = 0; ib < NCB; ++ib) {
+        if (ib >= nBi) break;
+        const double fab = fa * sB.scl[ib];
+        double* __restrict__ row = dst + (ra + sB.pos[ib]) * a.ncols;
+#pragma unroll
+        for (int ic = 0; ic < NCC; ++ic) {
+          if (ic >= nCi) break;
+          const double fabc = fab * sC.scl[ic];
+          double* __restrict__ rc = row + sC.pos[ic] * nDo;
+#pragma unroll
+          for (int id = 0; id < NCD; ++id) {
+            if (id >= nDi) break;
+            rc[sD.pos[id]] = out[((ia * NCB + ib) * NCC + ic) * NCD + id] * fabc * sD.scl[id];
+          }
+        }
+      }
+    }
+  }
+}
+
+}  // namespace gbx

@@ -1,0 +1,87 @@
+// Device data layout of the ERI engine (shared by all kernels and the C-ABI runtime).
+//
+// Terms: a "shell" here is a segmented contraction (one column m of a gbasis
+// GeneralizedContractionShell's coefficient matrix); a "pair" is an unordered pair of
+// shells stored with its higher-l shell first (A, then B); a "pair class" is (lA, lB);
+// a "class block" is the set of quartets (bra pair p, ket pair q) with
+// class(p) >= class(q), stored as a dense matrix of pair functions
+// rows = sum over pairs p of class(p) of nout(A_p)*nout(B_p), cols likewise for class(q).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gbx {
+
+constexpr int kLMax = 3;          // highest shell angular momentum the engine handles
+constexpr int kMaxCart = 10;      // (kLMax+1)(kLMax+2)/2
+constexpr int kBoysNGrid = 401;   // T_n = n / 10, n = 0..400
+constexpr double kBoysStep = 0.1;
+constexpr double kBoysTMax = 40.0;  // F_m(T) for T >= kBoysTMax by the asymptotic form
+constexpr int kBoysTaylor = 8;      // Taylor terms around the nearest grid point (|dT| <= 0.05)
+constexpr int kBoysMMax = 4 * kLMax + 1;  // highest Boys order any class needs (+1 spare)
+constexpr int kBoysOrders = kBoysMMax + kBoysTaylor;  // orders stored in the global table
+
+__host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+
+// Pair classes are ordered pair types (lA, lB), A being the shell the vertical recursion runs
+// on (the one with the larger exponent, for numerical stability), sorted by
+// (lA + lB, max(lA, lB), lA).  A quartet's bra is the pair with the larger class index.
+constexpr int kNumPairClasses = (kLMax + 1) * (kLMax + 1);
+constexpr int kPairClassL[kNumPairClasses][2] = {
+    {0, 0}, {0, 1}, {1, 0}, {1, 1}, {0, 2}, {2, 0}, {1, 2}, {2, 1},
+    {0, 3}, {3, 0}, {2, 2}, {1, 3}, {3, 1}, {2, 3}, {3, 2}, {3, 3}};
+constexpr int pair_class_index(int la, int lb) {
+  for (int c = 0; c < kNumPairClasses; ++c)
+    if (kPairClassL[c][0] == la && kPairClassL[c][1] == lb) return c;
+  return -1;
+}
+
+// One shell (segmented contraction).  `pos` / `scl` map the engine's internal component
+// index (canonical Cartesian order, or for spherical shells with l >= 2 the canonical
+// real-solid-harmonic order s_l..s_1, c_0..c_l) to the output function index inside the
+// shell and its scale (norm_cont, Cartesian component norm or sign of the label).
+struct ShellDev {
+  double x, y, z;
+  int l, nprim, prim_off, nout;
+  int func_off, sph, pad0, pad1;
+  double scl[kMaxCart];
+  int8_t pos[kMaxCart];
+  int8_t pad2[6];
+};
+
+// One primitive pair of a shell pair: zeta = a+b, P, X = P - A (A = first shell of the
+// pair), C = c_a c_b N_a N_b exp(-ab/zeta |AB|^2) * sqrt(2) pi^{5/4} / zeta.
+struct __align__(16) PrimPair {
+  double zeta, izeta, Px, Py, Pz, Xx, Xy, Xz, C, pad;
+};
+
+struct PairDev {
+  int shA, shB, prim_off, nprim;
+  int cls, local, fo, nB;  // class, index within class, pair-function offset in class, nout(B)
+  double ABx, ABy, ABz, pad;
+};
+
+// Per class block: where its quartets live in the work list and in the compact store.
+struct BlockDev {
+  long long base;   // element offset of the block matrix in the compact store
+  long long ncols;  // pair functions of the ket class
+  long long work_off, work_cap;
+};
+
+// Arguments of one class kernel launch.
+struct EriLaunch {
+  const int2* work;         // (bra pair, ket pair) per quartet of this block
+  const int* work_count;    // device counter (screened count) or nullptr
+  long long work_off, nwork;  // nwork = capacity; actual count read from work_count
+  const PairDev* pairs;
+  const PrimPair* prims;
+  const ShellDev* shells;
+  const double* boys_tab;   // [kBoysNGrid][kBoysOrders + 1], last column e^{-T_n}
+  double* out;              // compact store
+  long long base, ncols;
+  int mode;                 // 0 = write block, 1 = Schwarz diagonal (max |.| -> qout)
+  double* qout;             // per-pair Schwarz value (mode 1)
+  int* status;              // device error flag
+};
+
+}  // namespace gbx

@@ -1,0 +1,389 @@
+// Device pipeline of a full-tensor call:
+//   K1 pair_precompute   — primitive-pair data (zeta, P, P-A, K_AB x coefficients) in HBM
+//   K2 build_work        — Schwarz test + warp-ballot compaction into per-class-block
+//                          work lists (bra pair, ket pair), enumerated in sorted pair order
+//   K4/K5 eri_block_fp64 — class-templated quartet kernels (eri_kernels.cuh)
+//   K6 expand_full       — the 8-fold symmetric N^4 tensor from the compact store,
+//                          coalesced writes in chemist or physicist order
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "gbx_eri.h"
+#include "gbx_common.cuh"
+#include "runtime.h"
+
+namespace gbx {
+
+#define GBX_CUDA(call, what)              \
+  do {                                    \
+    int _s = cuda_status((call), (what)); \
+    if (_s != GBX_OK) return _s;          \
+  } while (0)
+
+// ------------------------------------------------------------------- K1
+// Reference: gbasis/integrals/_two_elec_int.py:306-322 (exponent sums, product centres,
+// relative coordinates) and :335-348, :528-547 (prefactor and primitive normalisation).
+__global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,
+                                const ShellDev* __restrict__ shells,
+                                const double* __restrict__ exps, const double* __restrict__ coefs,
+                                PrimPair* __restrict__ prims) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const PairDev P = pairs[p];
+  const ShellDev& A = shells[P.shA];
+  const ShellDev& B = shells[P.shB];
+  const double ab2 = P.ABx * P.ABx + P.ABy * P.ABy + P.ABz * P.ABz;
+  const double kpi = 5.914967172795613;  // sqrt(2) pi^{5/4}
+  for (int ia = 0; ia < A.nprim; ++ia) {
+    const double a = exps[A.prim_off + ia];
+    const double na = coefs[A.prim_off + ia] * pow(2.0 * a / 3.14159265358979323846, 0.75) *
+                      pow(4.0 * a, 0.5 * A.l);
+    for (int ib = 0; ib < B.nprim; ++ib) {
+      const double b = exps[B.prim_off + ib];
+      const double nb = coefs[B.prim_off + ib] * pow(2.0 * b / 3.14159265358979323846, 0.75) *
+                        pow(4.0 * b, 0.5 * B.l);
+      const double z = a + b, iz = 1.0 / z;
+      PrimPair r;
+      r.zeta = z;
+      r.izeta = iz;
+      r.Px = (a * A.x + b * B.x) * iz;
+      r.Py = (a * A.y + b * B.y) * iz;
+      r.Pz = (a * A.z + b * B.z) * iz;
+      r.Xx = r.Px - A.x;
+      r.Xy = r.Py - A.y;
+      r.Xz = r.Pz - A.z;
+      r.C = kpi * na * nb * exp(-a * b * iz * ab2) * iz;
+      r.pad = 0.0;
+      prims[P.prim_off + ia * B.nprim + ib] = r;
+    }
+  }
+}
+
+// ------------------------------------------------------------------- K2
+struct BuildBlock {
+  int pb0, nb, pk0, nk;
+  int tri, blk;
+  long long work_off, ncand;
+};
+
+__global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* __restrict__ bb,
+                           const double* __restrict__ qs, double tau, int2* __restrict__ work,
+                           int* __restrict__ counts) {
+  const int2 cm = cta_map[blockIdx.x];
+  const BuildBlock B = bb[cm.x];
+  const long long t = (long long)cm.y + threadIdx.x;
+  bool pass = false;
+  int p = 0, q = 0;
+  if (t < B.ncand) {
+    long long pl, ql;
+    if (B.tri) {
+      pl = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+      while (pl * (pl + 1) / 2 > t) --pl;
+      while ((pl + 1) * (pl + 2) / 2 <= t) ++pl;
+      ql = t - pl * (pl + 1) / 2;
+    } else {
+      pl = t / B.nk;
+      ql = t - pl * B.nk;
+    }
+    p = B.pb0 + (int)pl;
+    q = B.pk0 + (int)ql;
+    pass = (tau <= 0.0) || (qs[p] * qs[q] >= tau);
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, pass);
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0 && mask) base = atomicAdd(&counts[B.blk], __popc(mask));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (pass) {
+    const int rank = __popc(mask & ((1u << lane) - 1u));
+    work[B.work_off + base + rank] = make_int2(p, q);
+  }
+}
+
+// ------------------------------------------------------------------- K6
+struct ExpandArgs {
+  long long n;
+  int nsh, notation;
+  const int* fsh;
+  const int* fcomp;
+  const int* pair_of;
+  const int4* pinfo;  // (cls, local, fo, nB)
+  const BlockDev* blocks;
+  const double* compact;
+  double* out;
+};
+
+__device__ __forceinline__ long long pair_row(const ExpandArgs& e, int s1, int c1, int s2, int c2,
+                                              int4& info) {
+  const int pe = e.pair_of[s1 * e.nsh + s2];
+  info = e.pinfo[pe >> 1];
+  return (long long)info.z + ((pe & 1) ? (long long)c2 * info.w + c1 : (long long)c1 * info.w + c2);
+}
+
+__global__ void __launch_bounds__(256) expand_full(const ExpandArgs e) {
+  const int lane = threadIdx.x & 31;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const long long n = e.n;
+  const long long rows = n * n * n;
+  for (long long r = warp; r < rows; r += nwarps) {
+    const long long i0 = r / (n * n), i1 = (r / n) % n, i2 = r % n;
+    // chemist: (a,b,c) = (i0,i1,i2); physicist out[i,j,k,l] = (ik|jl): (a,b,c) = (i0,i2,i1)
+    const int a = (int)i0;
+    const int b = (int)(e.notation == GBX_PHYSICIST ? i2 : i1);
+    const int c = (int)(e.notation == GBX_PHYSICIST ? i1 : i2);
+    int4 ip;
+    const long long rowp = pair_row(e, e.fsh[a], e.fcomp[a], e.fsh[b], e.fcomp[b], ip);
+    const int sc = e.fsh[c], cc = e.fcomp[c];
+    double* __restrict__ orow = e.out + r * n;
+    for (int d = lane; d < n; d += 32) {
+      int4 iq;
+      const long long rowq = pair_row(e, sc, cc, e.fsh[d], e.fcomp[d], iq);
+      long long off;
+      if (ip.x > iq.x || (ip.x == iq.x && ip.y >= iq.y)) {
+        const BlockDev bk = e.blocks[ip.x * kNumPairClasses + iq.x];
+        off = bk.base + rowp * bk.ncols + rowq;
+      } else {
+        const BlockDev bk = e.blocks[iq.x * kNumPairClasses + ip.x];
+        off = bk.base + rowq * bk.ncols + rowp;
+      }
+      orow[d] = __ldg(e.compact + off);
+    }
+  }
+}
+
+// ------------------------------------------------------------------- host side
+static int num_sms(int device) {
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+  return v > 0 ? v : 1;
+}
+
+int upload_basis(Basis& B) {
+  const int n = (int)B.shells.size();
+  const int np = (int)B.pairs.size();
+  int s;
+  if ((s = B.alloc((void**)&B.d_shells, n * sizeof(ShellDev), "cudaMalloc(shells)"))) return s;
+  if ((s = B.alloc((void**)&B.d_pairs, np * sizeof(PairDev), "cudaMalloc(pairs)"))) return s;
+  if ((s = B.alloc((void**)&B.d_prims, B.n_prim_pairs * sizeof(PrimPair), "cudaMalloc(prims)")))
+    return s;
+  if ((s = B.alloc((void**)&B.d_exps, B.h_exps.size() * sizeof(double), "cudaMalloc(exps)")))
+    return s;
+  if ((s = B.alloc((void**)&B.d_coefs, B.h_coefs.size() * sizeof(double), "cudaMalloc(coefs)")))
+    return s;
+  if ((s = B.alloc((void**)&B.d_pair_of, (size_t)n * n * sizeof(int), "cudaMalloc(pair_of)")))
+    return s;
+  GBX_CUDA(cudaMemcpy(B.d_shells, B.shells.data(), n * sizeof(ShellDev), cudaMemcpyHostToDevice),
+           "upload shells");
+  GBX_CUDA(cudaMemcpy(B.d_pairs, B.pairs.data(), np * sizeof(PairDev), cudaMemcpyHostToDevice),
+           "upload pairs");
+  GBX_CUDA(cudaMemcpy(B.d_exps, B.h_exps.data(), B.h_exps.size() * sizeof(double),
+                      cudaMemcpyHostToDevice), "upload exps");
+  GBX_CUDA(cudaMemcpy(B.d_coefs, B.h_coefs.data(), B.h_coefs.size() * sizeof(double),
+                      cudaMemcpyHostToDevice), "upload coefs");
+  GBX_CUDA(cudaMemcpy(B.d_pair_of, B.pair_of.data(), (size_t)n * n * sizeof(int),
+                      cudaMemcpyHostToDevice), "upload pair_of");
+  pair_precompute<<<(np + 127) / 128, 128>>>(B.d_pairs, np, B.d_shells, B.d_exps, B.d_coefs,
+                                             B.d_prims);
+  GBX_CUDA(cudaGetLastError(), "pair_precompute launch");
+
+  // function tables
+  std::vector<int> fsh(B.nbf), fcomp(B.nbf);
+  for (int sh = 0; sh < n; ++sh)
+    for (int c = 0; c < B.shells[sh].nout; ++c) {
+      fsh[B.shells[sh].func_off + c] = sh;
+      fcomp[B.shells[sh].func_off + c] = c;
+    }
+  if ((s = B.alloc((void**)&B.d_func_shell, B.nbf * sizeof(int), "cudaMalloc(fsh)"))) return s;
+  if ((s = B.alloc((void**)&B.d_func_comp, B.nbf * sizeof(int), "cudaMalloc(fcomp)"))) return s;
+  GBX_CUDA(cudaMemcpy(B.d_func_shell, fsh.data(), B.nbf * sizeof(int), cudaMemcpyHostToDevice),
+           "upload fsh");
+  GBX_CUDA(cudaMemcpy(B.d_func_comp, fcomp.data(), B.nbf * sizeof(int), cudaMemcpyHostToDevice),
+           "upload fcomp");
+  if ((s = B.alloc((void**)&B.d_blocks, B.block_table.size() * sizeof(BlockDev),
+                   "cudaMalloc(blocks)")))
+    return s;
+  GBX_CUDA(cudaMemcpy(B.d_blocks, B.block_table.data(), B.block_table.size() * sizeof(BlockDev),
+                      cudaMemcpyHostToDevice), "upload blocks");
+
+  // work list + build map
+  if ((s = B.alloc((void**)&B.d_work, (size_t)B.n_quartets * sizeof(int2), "cudaMalloc(work)")))
+    return s;
+  const int nblk = (int)B.blocks.size();
+  if ((s = B.alloc((void**)&B.d_counts, (nblk + 4) * sizeof(int), "cudaMalloc(counts)"))) return s;
+  std::vector<BuildBlock> bb(nblk);
+  std::vector<int2> cmap;
+  for (int k = 0; k < nblk; ++k) {
+    const HostBlock& h = B.blocks[k];
+    bb[k] = BuildBlock{(int)B.class_first[h.cb], (int)h.nb, (int)B.class_first[h.ck], (int)h.nk,
+                       h.tri ? 1 : 0, k, h.dev.work_off, h.ncand};
+    for (long long c0 = 0; c0 < h.ncand; c0 += 256) cmap.push_back(make_int2(k, (int)c0));
+    if (h.ncand > (1LL << 31) - 256)
+      return set_error(GBX_ERR_UNSUPPORTED, "class block with %lld quartets exceeds the limit",
+                       h.ncand);
+  }
+  B.n_cta_build = (int)cmap.size();
+  void* dbb = nullptr;
+  if ((s = B.alloc(&dbb, nblk * sizeof(BuildBlock), "cudaMalloc(build blocks)"))) return s;
+  if ((s = B.alloc((void**)&B.d_cta_map, cmap.size() * sizeof(int2), "cudaMalloc(cta map)")))
+    return s;
+  GBX_CUDA(cudaMemcpy(dbb, bb.data(), nblk * sizeof(BuildBlock), cudaMemcpyHostToDevice),
+           "upload build blocks");
+  GBX_CUDA(cudaMemcpy(B.d_cta_map, cmap.data(), cmap.size() * sizeof(int2), cudaMemcpyHostToDevice),
+           "upload cta map");
+  B.d_build_blocks = dbb;
+
+  std::vector<int4> pinfo(np);
+  for (int p = 0; p < np; ++p)
+    pinfo[p] = make_int4(B.pairs[p].cls, B.pairs[p].local, B.pairs[p].fo, B.pairs[p].nB);
+  if ((s = B.alloc((void**)&B.d_pinfo, np * sizeof(int4), "cudaMalloc(pinfo)"))) return s;
+  GBX_CUDA(cudaMemcpy(B.d_pinfo, pinfo.data(), np * sizeof(int4), cudaMemcpyHostToDevice),
+           "upload pinfo");
+  if ((s = B.alloc((void**)&B.d_q, np * sizeof(double), "cudaMalloc(q)"))) return s;
+  if ((s = B.alloc((void**)&B.d_qscreen, np * sizeof(double), "cudaMalloc(qscreen)"))) return s;
+  if ((s = boys_table(B.device, &B.d_boys))) return s;
+  GBX_CUDA(cudaDeviceSynchronize(), "basis upload");
+  return GBX_OK;
+}
+
+static EriLaunch base_launch(Basis& B) {
+  EriLaunch a;
+  memset(&a, 0, sizeof(a));
+  a.pairs = B.d_pairs;
+  a.prims = B.d_prims;
+  a.shells = B.d_shells;
+  a.boys_tab = B.d_boys;
+  a.out = B.d_compact;
+  return a;
+}
+
+static int class_dims(int cls, int& la, int& lb) {
+  la = kPairClassL[cls][0];
+  lb = kPairClassL[cls][1];
+  return 0;
+}
+
+int ensure_schwarz(Basis& B, cudaStream_t st) {
+  if (B.schwarz_ready) return GBX_OK;
+  const int np = (int)B.pairs.size();
+  std::vector<int2> diag(np);
+  for (int p = 0; p < np; ++p) diag[p] = make_int2(p, p);
+  int2* d_diag = nullptr;
+  GBX_CUDA(cudaMalloc(&d_diag, np * sizeof(int2)), "cudaMalloc(schwarz work)");
+  GBX_CUDA(cudaMemcpyAsync(d_diag, diag.data(), np * sizeof(int2), cudaMemcpyHostToDevice, st),
+           "upload schwarz work");
+  const int nsm = num_sms(B.device);
+  for (int c = 0; c < kNumPairClasses; ++c) {
+    if (B.class_count[c] == 0) continue;
+    int la, lb;
+    class_dims(c, la, lb);
+    EriLaunch a = base_launch(B);
+    a.work = d_diag;
+    a.work_off = B.class_first[c];
+    a.nwork = B.class_count[c];
+    a.mode = 1;
+    a.qout = B.d_q;
+    const int grid = (int)std::min<long long>((a.nwork + 127) / 128, (long long)nsm * 8);
+    int s = launch_class(la, lb, la, lb, a, grid, st);
+    if (s) {
+      cudaFree(d_diag);
+      return s;
+    }
+  }
+  std::vector<double> q(np);
+  cudaError_t e1 = cudaMemcpyAsync(q.data(), B.d_q, np * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaError_t e2 = cudaStreamSynchronize(st);
+  cudaFree(d_diag);
+  GBX_CUDA(e1, "download schwarz bounds");
+  GBX_CUDA(e2, "schwarz bounds");
+  // bound of the original (generalized) shell pair: max over its segmented pairs
+  const int n = (int)B.shells.size();
+  std::vector<int> grp = B.group;
+  if ((int)grp.size() != n) {
+    grp.resize(n);
+    for (int i = 0; i < n; ++i) grp[i] = i;
+  }
+  int ng = 0;
+  for (int g : grp) ng = std::max(ng, g + 1);
+  std::vector<double> gmax((size_t)ng * ng, 0.0);
+  for (int p = 0; p < np; ++p) {
+    int ga = grp[B.pairs[p].shA], gb = grp[B.pairs[p].shB];
+    if (ga > gb) std::swap(ga, gb);
+    double& m = gmax[(size_t)ga * ng + gb];
+    m = std::max(m, q[p]);
+  }
+  B.h_q.resize(np);
+  for (int p = 0; p < np; ++p) {
+    int ga = grp[B.pairs[p].shA], gb = grp[B.pairs[p].shB];
+    if (ga > gb) std::swap(ga, gb);
+    B.h_q[p] = gmax[(size_t)ga * ng + gb];
+  }
+  GBX_CUDA(cudaMemcpy(B.d_qscreen, B.h_q.data(), np * sizeof(double), cudaMemcpyHostToDevice),
+           "upload screening bounds");
+  B.schwarz_ready = true;
+  return GBX_OK;
+}
+
+int run_compact(Basis& B, double tau, cudaStream_t st) {
+  int s;
+  if (tau > 0.0 && (s = ensure_schwarz(B, st))) return s;
+  if ((s = B.ensure_scratch(B.compact_elems, 0))) return s;
+  const int nblk = (int)B.blocks.size();
+  GBX_CUDA(cudaMemsetAsync(B.d_counts, 0, nblk * sizeof(int), st), "clear counts");
+  if (tau > 0.0) {
+    // screened-out quartets are zero in the output: clear the store first
+    GBX_CUDA(cudaMemsetAsync(B.d_compact, 0, B.compact_elems * sizeof(double), st),
+             "clear compact store");
+  }
+  if (B.profiling) cudaEventRecord(B.ev[0], st);
+  build_work<<<B.n_cta_build, 256, 0, st>>>(B.d_cta_map, (const BuildBlock*)B.d_build_blocks,
+                                            B.d_qscreen, tau, B.d_work, B.d_counts);
+  GBX_CUDA(cudaGetLastError(), "build_work launch");
+  if (B.profiling) cudaEventRecord(B.ev[1], st);
+  const int nsm = num_sms(B.device);
+  for (int k = 0; k < nblk; ++k) {
+    const HostBlock& h = B.blocks[k];
+    int la, lb, lc, ld;
+    class_dims(h.cb, la, lb);
+    class_dims(h.ck, lc, ld);
+    EriLaunch a = base_launch(B);
+    a.work = B.d_work;
+    a.work_count = B.d_counts + k;
+    a.work_off = h.dev.work_off;
+    a.nwork = h.ncand;
+    a.base = h.dev.base;
+    a.ncols = h.dev.ncols;
+    a.mode = 0;
+    const int grid = (int)std::min<long long>((h.ncand + 127) / 128, (long long)nsm * 8);
+    if ((s = launch_class(la, lb, lc, ld, a, grid, st))) return s;
+  }
+  return GBX_OK;
+}
+
+int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st) {
+  int s = run_compact(B, tau, st);
+  if (s) return s;
+  ExpandArgs e;
+  e.n = B.nbf;
+  e.nsh = (int)B.shells.size();
+  e.notation = notation;
+  e.fsh = B.d_func_shell;
+  e.fcomp = B.d_func_comp;
+  e.pair_of = B.d_pair_of;
+  e.pinfo = B.d_pinfo;
+  e.blocks = B.d_blocks;
+  e.compact = B.d_compact;
+  e.out = out;
+  const long long rows = (long long)B.nbf * B.nbf * B.nbf;
+  const int grid = (int)std::max<long long>(1, std::min<long long>((rows + 7) / 8,
+                                                                    (long long)num_sms(B.device) * 16));
+  if (B.profiling) cudaEventRecord(B.ev[2], st);
+  expand_full<<<grid, 256, 0, st>>>(e);
+  GBX_CUDA(cudaGetLastError(), "expand_full launch");
+  if (B.profiling) cudaEventRecord(B.ev[3], st);
+  return GBX_OK;
+}
+
+}  // namespace gbx

@@ -1,0 +1,413 @@
+// Host runtime + C ABI of the ERI engine: basis packing, pair/class bookkeeping, device
+// buffers, kernel launches (pair precompute, Schwarz/work-list compaction, class kernels,
+// full-tensor expansion) and error reporting.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gbx_eri.h"
+#include "gbx_common.cuh"
+#include "runtime.h"
+
+namespace gbx {
+
+// ------------------------------------------------------------------------- errors
+static thread_local std::string g_last_error;
+
+int set_error(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return GBX_OK;
+  if (e == cudaErrorMemoryAllocation)
+    return set_error(GBX_ERR_OOM, "%s: %s", what, cudaGetErrorString(e));
+  return set_error(GBX_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define GBX_CUDA(call, what)                        \
+  do {                                              \
+    int _s = cuda_status((call), (what));           \
+    if (_s != GBX_OK) return _s;                    \
+  } while (0)
+
+// ------------------------------------------------------------------ Boys table
+// F_m(T) = e^{-T} sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1)): every term is positive, so
+// the sum in long double is accurate to ~1e-18 relative for the whole grid.
+static long double boys_series(int m, long double T) {
+  long double term = 1.0L / (2 * m + 1), sum = term;
+  for (int k = 1; k < 4000; ++k) {
+    term *= 2.0L * T / (2 * m + 2 * k + 1);
+    sum += term;
+    if (term < sum * 1e-22L) break;
+  }
+  return expl(-T) * sum;
+}
+
+static std::mutex g_boys_mu;
+static double* g_boys_dev[64] = {nullptr};
+
+int boys_table(int device, const double** out) {
+  std::lock_guard<std::mutex> lk(g_boys_mu);
+  if (device < 0 || device >= 64) return set_error(GBX_ERR_INVALID, "bad device %d", device);
+  if (!g_boys_dev[device]) {
+    std::vector<double> h((size_t)kBoysNGrid * (kBoysOrders + 1));
+    for (int n = 0; n < kBoysNGrid; ++n) {
+      const long double T = (long double)n / 10.0L;
+      for (int m = 0; m < kBoysOrders; ++m)
+        h[(size_t)n * (kBoysOrders + 1) + m] = (double)boys_series(m, T);
+      h[(size_t)n * (kBoysOrders + 1) + kBoysOrders] = (double)expl(-T);
+    }
+    double* d = nullptr;
+    GBX_CUDA(cudaMalloc(&d, h.size() * sizeof(double)), "cudaMalloc(boys table)");
+    GBX_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice),
+             "upload boys table");
+    g_boys_dev[device] = d;
+  }
+  *out = g_boys_dev[device];
+  return GBX_OK;
+}
+
+// ------------------------------------------------------------------ basis setup
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+static void free_dev(void* p) {
+  if (p) cudaFree(p);
+}
+
+Basis::~Basis() {
+  DeviceGuard g(device);
+  for (void* p : dev_allocs) free_dev(p);
+  for (cudaEvent_t& e : ev)
+    if (e) cudaEventDestroy(e);
+}
+
+int Basis::alloc(void** p, size_t bytes, const char* what) {
+  if (bytes == 0) bytes = 16;
+  GBX_CUDA(cudaMalloc(p, bytes), what);
+  dev_allocs.push_back(*p);
+  return GBX_OK;
+}
+
+int Basis::ensure_scratch(size_t compact_elems, size_t work_elems) {
+  if (compact_elems > compact_cap) {
+    if (d_compact) {
+      cudaFree(d_compact);
+      dev_allocs.erase(std::find(dev_allocs.begin(), dev_allocs.end(), (void*)d_compact));
+      d_compact = nullptr;
+    }
+    int s = alloc((void**)&d_compact, compact_elems * sizeof(double), "cudaMalloc(compact store)");
+    if (s) return s;
+    compact_cap = compact_elems;
+  }
+  (void)work_elems;
+  return GBX_OK;
+}
+
+static int build_basis(Basis& B, int n, const int* angmom, const int* nprim, const double* center,
+                       const double* exps, const double* coefs, const int* nout, const int* sph,
+                       const int8_t* pos, const double* scl) {
+  B.shells.resize(n);
+  int prim_total = 0, func = 0;
+  for (int s = 0; s < n; ++s) {
+    if (angmom[s] < 0) return set_error(GBX_ERR_INVALID, "shell %d: negative angmom", s);
+    if (angmom[s] > B.lmax_supported)
+      return set_error(GBX_ERR_UNSUPPORTED,
+                       "shell %d: angular momentum %d above the compiled maximum %d", s,
+                       angmom[s], B.lmax_supported);
+    if (nprim[s] <= 0) return set_error(GBX_ERR_INVALID, "shell %d: no primitives", s);
+    const int nint = (sph[s] && angmom[s] >= 2) ? 2 * angmom[s] + 1 : ncart(angmom[s]);
+    if (nout[s] != nint)
+      return set_error(GBX_ERR_INVALID, "shell %d: nout %d, expected %d", s, nout[s], nint);
+    ShellDev& d = B.shells[s];
+    memset(&d, 0, sizeof(d));
+    d.x = center[3 * s];
+    d.y = center[3 * s + 1];
+    d.z = center[3 * s + 2];
+    d.l = angmom[s];
+    d.nprim = nprim[s];
+    d.prim_off = prim_total;
+    d.nout = nout[s];
+    d.func_off = func;
+    d.sph = sph[s] ? 1 : 0;
+    for (int c = 0; c < kMaxCart; ++c) {
+      d.scl[c] = scl[kMaxCart * s + c];
+      d.pos[c] = pos[kMaxCart * s + c];
+    }
+    for (int c = 0; c < nint; ++c)
+      if (d.pos[c] < 0 || d.pos[c] >= nout[s])
+        return set_error(GBX_ERR_INVALID, "shell %d: component %d maps outside the shell", s, c);
+    for (int k = 0; k < nprim[s]; ++k)
+      if (!(exps[prim_total + k] > 0.0))
+        return set_error(GBX_ERR_INVALID, "shell %d: exponents must be positive", s);
+    prim_total += nprim[s];
+    func += nout[s];
+  }
+  B.nbf = func;
+  B.h_exps.assign(exps, exps + prim_total);
+  B.h_coefs.assign(coefs, coefs + prim_total);
+
+  // pairs: i <= j, stored with the shell of larger maximum exponent first (the vertical
+  // recursion runs on it: P - A stays small, which keeps the Obara-Saika and transfer
+  // recursions from cancelling digits on diffuse partners); ties: higher l, lower index.
+  // Sorted by (class, nprim desc).
+  struct HP {
+    int a, b, cls, nprim, i, j;
+  };
+  std::vector<double> emax(n, 0.0);
+  for (int s2 = 0, off = 0; s2 < n; off += nprim[s2], ++s2)
+    for (int k = 0; k < nprim[s2]; ++k) emax[s2] = std::max(emax[s2], exps[off + k]);
+  std::vector<HP> hp;
+  hp.reserve((size_t)n * (n + 1) / 2);
+  for (int i = 0; i < n; ++i)
+    for (int j = i; j < n; ++j) {
+      int a = i, b = j;
+      if (emax[j] > emax[i] || (emax[j] == emax[i] && angmom[j] > angmom[i])) std::swap(a, b);
+      hp.push_back({a, b, pair_class_index(angmom[a], angmom[b]), nprim[a] * nprim[b], i, j});
+    }
+  std::stable_sort(hp.begin(), hp.end(), [](const HP& x, const HP& y) {
+    if (x.cls != y.cls) return x.cls < y.cls;
+    return x.nprim > y.nprim;
+  });
+  const int np = (int)hp.size();
+  B.pairs.resize(np);
+  B.pair_of.assign((size_t)n * n, -1);
+  B.class_first.assign(kNumPairClasses + 1, 0);
+  B.class_count.assign(kNumPairClasses, 0);
+  B.class_funcs.assign(kNumPairClasses, 0);
+  long long prim_pairs = 0;
+  for (int p = 0; p < np; ++p) {
+    const HP& h = hp[p];
+    PairDev& d = B.pairs[p];
+    memset(&d, 0, sizeof(d));
+    d.shA = h.a;
+    d.shB = h.b;
+    d.prim_off = (int)prim_pairs;
+    d.nprim = h.nprim;
+    d.cls = h.cls;
+    d.local = B.class_count[h.cls]++;
+    d.fo = (int)B.class_funcs[h.cls];
+    d.nB = B.shells[h.b].nout;
+    B.class_funcs[h.cls] += (long long)B.shells[h.a].nout * B.shells[h.b].nout;
+    d.ABx = B.shells[h.a].x - B.shells[h.b].x;
+    d.ABy = B.shells[h.a].y - B.shells[h.b].y;
+    d.ABz = B.shells[h.a].z - B.shells[h.b].z;
+    prim_pairs += h.nprim;
+    // orientation bit: 1 if the first function index of the ordered pair (i,j) lives
+    // on the pair's B shell
+    B.pair_of[(size_t)h.a * n + h.b] = p << 1;
+    if (h.a != h.b) B.pair_of[(size_t)h.b * n + h.a] = (p << 1) | 1;
+  }
+  for (int c = 0; c < kNumPairClasses; ++c) B.class_first[c + 1] = B.class_first[c] + B.class_count[c];
+  B.n_prim_pairs = prim_pairs;
+
+  // class blocks (cb >= ck) that have quartets
+  B.blocks.clear();
+  B.block_table.assign((size_t)kNumPairClasses * kNumPairClasses, BlockDev{-1, 0, 0, 0});
+  long long base = 0, work = 0;
+  for (int cb = 0; cb < kNumPairClasses; ++cb)
+    for (int ck = 0; ck <= cb; ++ck) {
+      const long long nb = B.class_count[cb], nk = B.class_count[ck];
+      if (nb == 0 || nk == 0) continue;
+      HostBlock hb;
+      hb.cb = cb;
+      hb.ck = ck;
+      hb.nb = nb;
+      hb.nk = nk;
+      hb.tri = (cb == ck);
+      hb.ncand = hb.tri ? nb * (nb + 1) / 2 : nb * nk;
+      hb.dev.base = base;
+      hb.dev.ncols = B.class_funcs[ck];
+      hb.dev.work_off = work;
+      hb.dev.work_cap = hb.ncand;
+      base += B.class_funcs[cb] * B.class_funcs[ck];
+      work += hb.ncand;
+      B.block_table[(size_t)cb * kNumPairClasses + ck] = hb.dev;
+      B.blocks.push_back(hb);
+    }
+  B.compact_elems = base;
+  B.n_quartets = work;
+  return GBX_OK;
+}
+
+}  // namespace gbx
+
+using namespace gbx;
+
+struct gbx_basis {
+  std::unique_ptr<Basis> impl;
+};
+
+extern "C" {
+
+int gbx_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return GBX_ERR_INVALID;
+  snprintf(buf, len, "%s", g_last_error.c_str());
+  return GBX_OK;
+}
+
+int gbx_basis_create(gbx_basis** out, int n_shells, const int* angmom, const int* nprim,
+                     const double* center, const double* exps, const double* coefs,
+                     const int* nout, const int* sph, const int8_t* pos, const double* scl,
+                     int device) {
+  if (!out || n_shells <= 0 || !angmom || !nprim || !center || !exps || !coefs || !nout ||
+      !sph || !pos || !scl)
+    return set_error(GBX_ERR_INVALID, "gbx_basis_create: null argument or empty basis");
+  *out = nullptr;
+  int ndev = 0;
+  GBX_CUDA(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+  if (device < 0 || device >= ndev)
+    return set_error(GBX_ERR_INVALID, "device %d not present (%d devices)", device, ndev);
+  auto B = std::make_unique<Basis>();
+  B->device = device;
+  B->lmax_supported = compiled_lmax();
+  int s = build_basis(*B, n_shells, angmom, nprim, center, exps, coefs, nout, sph, pos, scl);
+  if (s) return s;
+  DeviceGuard g(device);
+  s = upload_basis(*B);
+  if (s) return s;
+  *out = new gbx_basis{std::move(B)};
+  return GBX_OK;
+}
+
+int gbx_basis_destroy(gbx_basis* b) {
+  delete b;
+  return GBX_OK;
+}
+
+int gbx_basis_nbf(const gbx_basis* b, int64_t* nbf) {
+  if (!b || !nbf) return set_error(GBX_ERR_INVALID, "gbx_basis_nbf: null argument");
+  *nbf = b->impl->nbf;
+  return GBX_OK;
+}
+
+int gbx_basis_stats(const gbx_basis* b, int64_t* n_quartets, int64_t* compact_bytes) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_basis_stats: null basis");
+  if (n_quartets) *n_quartets = b->impl->n_quartets;
+  if (compact_bytes) *compact_bytes = b->impl->compact_elems * (int64_t)sizeof(double);
+  return GBX_OK;
+}
+
+int gbx_eri_full(gbx_basis* b, int notation, double tau, double* out, void* stream) {
+  if (!b || !out) return set_error(GBX_ERR_INVALID, "gbx_eri_full: null argument");
+  if (notation != GBX_CHEMIST && notation != GBX_PHYSICIST)
+    return set_error(GBX_ERR_INVALID, "notation must be GBX_CHEMIST or GBX_PHYSICIST");
+  if (!(tau >= 0.0)) return set_error(GBX_ERR_INVALID, "schwarz threshold must be >= 0");
+  Basis& B = *b->impl;
+  DeviceGuard g(B.device);
+  return run_full(B, notation, tau, out, (cudaStream_t)stream);
+}
+
+int gbx_eri_full_host(gbx_basis* b, int notation, double tau, double* out_host, void* stream) {
+  if (!b || !out_host) return set_error(GBX_ERR_INVALID, "gbx_eri_full_host: null argument");
+  Basis& B = *b->impl;
+  DeviceGuard g(B.device);
+  const size_t n4 = (size_t)B.nbf * B.nbf * B.nbf * B.nbf;
+  if (n4 > B.out_cap) {
+    if (B.d_out) {
+      cudaFree(B.d_out);
+      B.dev_allocs.erase(std::find(B.dev_allocs.begin(), B.dev_allocs.end(), (void*)B.d_out));
+      B.d_out = nullptr;
+    }
+    int s = B.alloc((void**)&B.d_out, n4 * sizeof(double), "cudaMalloc(full tensor)");
+    if (s) return s;
+    B.out_cap = n4;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  int s = gbx_eri_full(b, notation, tau, B.d_out, stream);
+  if (s) return s;
+  GBX_CUDA(cudaMemcpyAsync(out_host, B.d_out, n4 * sizeof(double), cudaMemcpyDeviceToHost, st),
+           "copy tensor to host");
+  GBX_CUDA(cudaStreamSynchronize(st), "synchronize");
+  return GBX_OK;
+}
+
+int gbx_schwarz_bounds(gbx_basis* b, double* q_host) {
+  if (!b || !q_host) return set_error(GBX_ERR_INVALID, "gbx_schwarz_bounds: null argument");
+  Basis& B = *b->impl;
+  DeviceGuard g(B.device);
+  int s = ensure_schwarz(B, nullptr);
+  if (s) return s;
+  const int n = (int)B.shells.size();
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      const int pe = B.pair_of[(size_t)i * n + j];
+      q_host[(size_t)i * n + j] = B.h_q[pe >> 1];
+    }
+  return GBX_OK;
+}
+
+int gbx_set_profiling(gbx_basis* b, int on) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_set_profiling: null basis");
+  Basis& B = *b->impl;
+  DeviceGuard g(B.device);
+  if (on && !B.ev[0])
+    for (cudaEvent_t& e : B.ev) GBX_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+  B.profiling = on != 0;
+  return GBX_OK;
+}
+
+int gbx_phase_times(gbx_basis* b, double* ms) {
+  if (!b || !ms) return set_error(GBX_ERR_INVALID, "gbx_phase_times: null argument");
+  Basis& B = *b->impl;
+  if (!B.profiling) return set_error(GBX_ERR_INVALID, "profiling is off for this basis");
+  DeviceGuard g(B.device);
+  GBX_CUDA(cudaEventSynchronize(B.ev[3]), "phase events");
+  for (int i = 0; i < 3; ++i) {
+    float t = 0.f;
+    GBX_CUDA(cudaEventElapsedTime(&t, B.ev[i], B.ev[i + 1]), "phase elapsed time");
+    ms[i] = t;
+  }
+  return GBX_OK;
+}
+
+int gbx_basis_set_groups(gbx_basis* b, const int* group) {
+  if (!b || !group) return set_error(GBX_ERR_INVALID, "gbx_basis_set_groups: null argument");
+  Basis& B = *b->impl;
+  const int n = (int)B.shells.size();
+  B.group.assign(group, group + n);
+  for (int i = 0; i < n; ++i)
+    if (group[i] < 0) return set_error(GBX_ERR_INVALID, "negative shell group");
+  B.schwarz_ready = false;
+  return GBX_OK;
+}
+
+int gbx_last_counts(const gbx_basis* b, int64_t* computed, int64_t* screened) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_last_counts: null basis");
+  Basis& B = *b->impl;
+  DeviceGuard g(B.device);
+  const int nblk = (int)B.blocks.size();
+  std::vector<int> c(nblk);
+  GBX_CUDA(cudaMemcpy(c.data(), B.d_counts, nblk * sizeof(int), cudaMemcpyDeviceToHost),
+           "read quartet counters");
+  long long tot = 0;
+  for (int v : c) tot += v;
+  if (computed) *computed = tot;
+  if (screened) *screened = B.n_quartets - tot;
+  return GBX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,80 @@
+// Host-side state of a basis handle (internal to libgbx_eri).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "errors.h"
+#include "gbx_common.cuh"
+#include "gbx_eri.h"
+
+namespace gbx {
+
+int boys_table(int device, const double** out);
+int compiled_lmax();
+
+struct HostBlock {
+  int cb, ck;
+  long long nb, nk, ncand;
+  bool tri;
+  BlockDev dev;
+};
+
+struct Basis {
+  int device = 0;
+  int lmax_supported = 0;
+  long long nbf = 0;
+  std::vector<ShellDev> shells;
+  std::vector<double> h_exps, h_coefs;
+  std::vector<PairDev> pairs;
+  std::vector<int> pair_of;  // n*n: (pair << 1) | (first index on B shell)
+  std::vector<int> group;    // original (generalized) shell of each segmented shell
+  std::vector<long long> class_first, class_count, class_funcs;
+  std::vector<HostBlock> blocks;
+  std::vector<BlockDev> block_table;  // kNumPairClasses^2, base = -1 when empty
+  long long compact_elems = 0, n_quartets = 0, n_prim_pairs = 0;
+
+  // device copies
+  ShellDev* d_shells = nullptr;
+  PairDev* d_pairs = nullptr;
+  PrimPair* d_prims = nullptr;
+  double* d_exps = nullptr;
+  double* d_coefs = nullptr;
+  int* d_pair_of = nullptr;
+  int* d_func_shell = nullptr;
+  int* d_func_comp = nullptr;
+  BlockDev* d_blocks = nullptr;
+  int2* d_work = nullptr;
+  int* d_counts = nullptr;  // per block screened count + status words
+  double* d_q = nullptr;    // per-pair Schwarz bound (segmented)
+  double* d_qscreen = nullptr;  // per-pair bound of the original shell pair
+  int2* d_cta_map = nullptr;    // work-list build: (block, first candidate) per CTA
+  void* d_build_blocks = nullptr;
+  int4* d_pinfo = nullptr;      // per pair (cls, local, fo, nB) for the expansion
+  int n_cta_build = 0;
+  const double* d_boys = nullptr;
+  double* d_compact = nullptr;
+  size_t compact_cap = 0;
+  double* d_out = nullptr;
+  size_t out_cap = 0;
+  bool schwarz_ready = false;
+  std::vector<double> h_q;  // per pair, original-shell-pair bound
+  long long last_computed = 0, last_screened = 0;
+  // optional phase timing with events on the launching stream:
+  // [0] work-list build, [1] class kernels, [2] expansion
+  bool profiling = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<void*> dev_allocs;
+
+  ~Basis();
+  int alloc(void** p, size_t bytes, const char* what);
+  int ensure_scratch(size_t compact_elems, size_t work_elems);
+};
+
+int upload_basis(Basis& B);
+int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st);
+int run_compact(Basis& B, double tau, cudaStream_t st);
+int ensure_schwarz(Basis& B, cudaStream_t st);
+int launch_class(int la, int lb, int lc, int ld, const EriLaunch& a, int grid, cudaStream_t st);
+
+}  // namespace gbx

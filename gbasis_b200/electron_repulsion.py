@@ -1,0 +1,204 @@
+"""Drop-in for ``gbasis.integrals.electron_repulsion`` backed by the B200 engine.
+
+Same entry points, arguments, array layouts and errors as the reference:
+
+* :func:`electron_repulsion_integral` (``gbasis/integrals/electron_repulsion.py:214-281``);
+* :class:`ElectronRepulsionIntegral` with ``construct_array_contraction`` (classmethod,
+  ``:86-211``) and ``construct_array_{cartesian,spherical,mix,lincomb}``
+  (``gbasis/base_four_symm.py:160-616``);
+* :func:`electron_repulsion_integral_improved` with ``schwarz_threshold``
+  (``electron_repulsion.py:415-504``).
+
+Every array is computed on the GPU by ``libgbx_eri.so`` through its C ABI; there is no CPU
+path (a missing library or device raises).  The chemist-order tensor is produced
+contiguously and the physicist result is the reference's ``transpose(0, 2, 1, 3)`` view.
+Extras are keyword-only: ``coord_type`` (overrides every shell's ``coord_type``),
+``device`` and ``out`` (a preallocated C-contiguous float64 array, e.g. page-locked).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _engine
+from .contractions import is_shell
+
+__all__ = ["ElectronRepulsionIntegral", "ElectronRepulsionIntegralImproved",
+           "electron_repulsion_integral", "electron_repulsion_integral_improved"]
+
+
+def _boys_host(orders, weighted_dist, rho=None):
+    """F_m(T) = 1F1(m+1/2; m+3/2; -T)/(2m+1) on the host.  Kept as the ``boys_func`` class
+    attribute for API compatibility (``electron_repulsion.py:84``); the device engine uses its
+    own tabulated Boys function and does not call this."""
+    from scipy.special import hyp1f1
+    orders = np.asarray(orders)
+    return hyp1f1(orders + 0.5, orders + 1.5, -np.asarray(weighted_dist)) / (2 * orders + 1)
+
+
+def _check_contractions(contractions):
+    # gbasis/base.py:32-65
+    if not isinstance(contractions, (list, tuple)):
+        raise TypeError("Contractions must be given as a list or tuple of "
+                        "`GeneralizedContractionShell` instance")
+    if not contractions:
+        raise ValueError("At least one `GeneralizedContractionShell` must be given.")
+    for c in contractions:
+        if not is_shell(c):
+            raise TypeError("Given contractions must be instances of the "
+                            "`GeneralizedContractionShell` class.")
+
+
+def _norm_types(coord_types, n):
+    if not isinstance(coord_types, (list, tuple)):
+        raise TypeError("`coord_types` must be a list or a tuple.")
+    if not all(i in ["cartesian", "spherical"] for i in coord_types):
+        raise ValueError("Each entry of `coord_types` must be one of 'cartesian' or 'spherical'.")
+    if len(coord_types) != n:
+        raise ValueError("`coord_types` must have the same number of entries as the number of "
+                         "`GeneralizedContractionShell` in the instance.")
+    return list(coord_types)
+
+
+class ElectronRepulsionIntegral:
+    """Electron-repulsion integrals of a basis, chemist notation (``(ab|cd)``)."""
+
+    boys_func = staticmethod(_boys_host)
+    _screen = 0.0
+
+    def __init__(self, contractions):
+        _check_contractions(contractions)
+        self._axes_contractions = (tuple(contractions),)
+
+    @property
+    def contractions(self):
+        return self._axes_contractions[0]
+
+    # ------------------------------------------------------------------ per quartet
+    @classmethod
+    def construct_array_contraction(cls, cont_one, cont_two, cont_three, cont_four):
+        """(M1, L1, M2, L2, M3, L3, M4, L4) block of four shells, Cartesian, primitive and
+        component norms applied, ``norm_cont`` not applied (``electron_repulsion.py:86-211``).
+        Computed on the device as a batch of one."""
+        for name, c in (("cont_one", cont_one), ("cont_two", cont_two),
+                        ("cont_three", cont_three), ("cont_four", cont_four)):
+            if not is_shell(c):
+                raise TypeError(f"`{name}` must be a `GeneralizedContractionShell` instance.")
+        shells = [cont_one, cont_two, cont_three, cont_four]
+        db = _engine.DeviceBasis(shells, raw=True)
+        full = db.full_host("chemist")
+        db.close()
+        dims = []
+        for s in shells:
+            c = np.asarray(s.coeffs)
+            dims.append((c.shape[1] if c.ndim == 2 else 1, len(s.angmom_components_cart)))
+        off = np.cumsum([0] + [m * l for m, l in dims])
+        blk = full[off[0]:off[1], off[1]:off[2], off[2]:off[3], off[3]:off[4]]
+        return np.ascontiguousarray(blk).reshape(
+            dims[0][0], dims[0][1], dims[1][0], dims[1][1], dims[2][0], dims[2][1],
+            dims[3][0], dims[3][1])
+
+    # ---------------------------------------------------------------- whole basis
+    def _full(self, coord_types, out=None, device=None):
+        db = _engine.DeviceBasis(list(self.contractions), coord_types, device=device)
+        try:
+            return db.full_host("chemist", self._screen, out=out)
+        finally:
+            db.close()
+
+    def construct_array_cartesian(self, out=None, device=None):
+        return self._full(["cartesian"] * len(self.contractions), out, device)
+
+    def construct_array_spherical(self, out=None, device=None):
+        return self._full(["spherical"] * len(self.contractions), out, device)
+
+    def construct_array_mix(self, coord_types, out=None, device=None):
+        return self._full(_norm_types(coord_types, len(self.contractions)), out, device)
+
+    def construct_array_lincomb(self, transform, coord_type, device=None):
+        """``base_four_symm.py:559-616``: ERI tensor in the given coordinate types, then the
+        four-index transform on the device (cuBLAS DGEMM chain)."""
+        if all(ct == "cartesian" for ct in coord_type):
+            types = ["cartesian"] * len(self.contractions)
+        elif all(ct == "spherical" for ct in coord_type):
+            types = ["spherical"] * len(self.contractions)
+        elif isinstance(coord_type, (list, tuple)):
+            types = _norm_types(coord_type, len(self.contractions))
+        else:
+            raise TypeError("`coord_type` must be a list/tuple of the strings 'cartesian' or "
+                            "'spherical'")
+        return _lincomb_device(list(self.contractions), types, np.asarray(transform, dtype=float),
+                               self._screen, device)
+
+
+class ElectronRepulsionIntegralImproved(ElectronRepulsionIntegral):
+    """Same integrals; ``schwarz_threshold`` zeroes quartets with Q_ij Q_kl below it."""
+
+    def __init__(self, contractions, schwarz_threshold=0.0):
+        super().__init__(contractions)
+        self._screen = float(schwarz_threshold)
+
+
+def _lincomb_device(shells, types, transform, screen, device):
+    import ctypes
+    import torch
+    db = _engine.DeviceBasis(shells, types, device=device)
+    try:
+        n = db.nbf
+        if transform.ndim != 2 or transform.shape[1] != n:
+            raise ValueError(f"`transform` must have shape (K, {n})")
+        k = transform.shape[0]
+        dev = torch.device("cuda", db.device)
+        m = max(n, k)
+        eri = torch.empty(n ** 4, dtype=torch.float64, device=dev)
+        work = torch.empty(2 * m ** 4, dtype=torch.float64, device=dev)
+        out = torch.empty(k ** 4, dtype=torch.float64, device=dev)
+        T = torch.from_numpy(np.ascontiguousarray(transform)).to(dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        db.full_device(eri.data_ptr(), "chemist", screen, stream=ctypes.c_void_p(stream))
+        _engine.check(_engine.lib().gbx_lincomb(
+            ctypes.c_void_p(eri.data_ptr()), n, ctypes.c_void_p(T.data_ptr()), k,
+            ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(work.data_ptr()),
+            ctypes.c_void_p(stream)), "gbx_lincomb")
+        return out.cpu().numpy().reshape(k, k, k, k)
+    finally:
+        db.close()
+
+
+def _dispatch(cls_obj, basis, transform, coord_type, out, device):
+    types = [{"c": "cartesian", "p": "spherical"}.get(s.coord_type, s.coord_type) for s in basis]
+    if coord_type is not None:
+        types = [coord_type] * len(basis) if isinstance(coord_type, str) else list(coord_type)
+    if transform is not None:
+        return cls_obj.construct_array_lincomb(transform, types, device=device)
+    if all(ct == "cartesian" for ct in types):
+        return cls_obj.construct_array_cartesian(out=out, device=device)
+    if all(ct == "spherical" for ct in types):
+        return cls_obj.construct_array_spherical(out=out, device=device)
+    return cls_obj.construct_array_mix(types, out=out, device=device)
+
+
+def electron_repulsion_integral(basis, transform=None, notation="physicist", *, coord_type=None,
+                                device=None, out=None):
+    """ERIs of ``basis`` (``electron_repulsion.py:214-281``): (K, K, K, K) float64, physicist
+    notation by default (a ``transpose(0, 2, 1, 3)`` view of the chemist array)."""
+    if notation not in ["physicist", "chemist"]:
+        raise ValueError("`notation` must be one of 'physicist' or 'chemist'")
+    array = _dispatch(ElectronRepulsionIntegral(basis), basis, transform, coord_type, out, device)
+    if notation == "physicist":
+        array = np.transpose(array, (0, 2, 1, 3))
+    return array
+
+
+def electron_repulsion_integral_improved(basis, transform=None, notation="physicist",
+                                         schwarz_threshold=0.0, *, coord_type=None, device=None,
+                                         out=None):
+    """``electron_repulsion.py:415-504``: as :func:`electron_repulsion_integral`, with shell
+    quartets whose Schwarz bound Q_ij Q_kl (blocks without ``norm_cont``) is below
+    ``schwarz_threshold`` set to zero."""
+    if notation not in ["physicist", "chemist"]:
+        raise ValueError("`notation` must be one of 'physicist' or 'chemist'")
+    obj = ElectronRepulsionIntegralImproved(basis, schwarz_threshold)
+    array = _dispatch(obj, basis, transform, coord_type, out, device)
+    if notation == "physicist":
+        array = np.transpose(array, (0, 2, 1, 3))
+    return array

@@ -1,0 +1,126 @@
+/*
+ * gbx_eri.h — C ABI of the B200 electron-repulsion-integral engine (libgbx_eri.so).
+ *
+ * Plain C types only: the caller passes host arrays describing the basis, and device or
+ * host pointers for outputs.  Every function returns a status code (GBX_OK = 0); the
+ * message of the last failure on the calling thread is available from gbx_last_error().
+ *
+ * Reference interfaces these entry points replace (paths inside theochem/gbasis):
+ *   - gbx_basis_create           <- GeneralizedContractionShell objects handed to
+ *                                   ElectronRepulsionIntegral(basis)
+ *                                   (gbasis/integrals/electron_repulsion.py:20,
+ *                                    gbasis/base.py:32-65, gbasis/contractions.py:118)
+ *   - gbx_eri_full / _full_host  <- electron_repulsion_integral(basis, transform=None,
+ *                                   notation=...) and BaseFourIndexSymmetric
+ *                                   .construct_array_{cartesian,spherical,mix}
+ *                                   (gbasis/integrals/electron_repulsion.py:214-281,
+ *                                    gbasis/base_four_symm.py:160-557)
+ *   - gbx_eri_full with a Schwarz threshold
+ *                                <- electron_repulsion_integral_improved(...,
+ *                                   schwarz_threshold) (electron_repulsion.py:415-504,
+ *                                   gbasis/integrals/_schwarz_screening.py:131-191)
+ *   - gbx_schwarz_bounds         <- compute_schwarz_bounds (_schwarz_screening.py:62-90)
+ *   - gbx_lincomb                <- construct_array_lincomb's four tensordots
+ *                                   (gbasis/base_four_symm.py:559-616)
+ *   - gbx_eri_coulomb_j          <- (no direct counterpart: J_ab = sum_cd (ab|cd) D_cd,
+ *                                   the contraction gbasis users apply to the tensor)
+ */
+#ifndef GBX_ERI_H
+#define GBX_ERI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  GBX_OK = 0,
+  GBX_ERR_INVALID = 1,     /* bad argument (shape, value, null pointer) */
+  GBX_ERR_UNSUPPORTED = 2, /* angular momentum above the compiled maximum */
+  GBX_ERR_OOM = 3,         /* device allocation failed */
+  GBX_ERR_CUDA = 4,        /* CUDA runtime / launch error */
+  GBX_ERR_TIMEOUT = 5      /* a bounded device wait gave up */
+};
+
+/* Output layout of full-tensor calls. */
+enum { GBX_CHEMIST = 0, GBX_PHYSICIST = 1 };
+
+typedef struct gbx_basis gbx_basis;
+
+/*
+ * Describe a basis of n_shells segmented contractions (one per column of a gbasis
+ * coefficient matrix, in basis-function order).  Per shell s:
+ *   angmom[s], nprim[s], center[3s..3s+2];
+ *   exps / coefs: nprim[s] values each, concatenated over shells (raw contraction
+ *     coefficients; primitive normalisation is applied by the engine);
+ *   nout[s]: output functions of the shell (L_cart or 2l+1);
+ *   sph[s]: 1 if the shell is transformed to real solid harmonics;
+ *   pos[10s..]: for each engine-internal component (canonical Cartesian order, or for
+ *     spherical shells with l >= 2 the order s_l..s_1, c_0..c_l) the output position
+ *     within the shell, or -1;
+ *   scl[10s..]: matching scale (norm_cont x component norm or sign).
+ * device: CUDA ordinal the basis lives on.
+ */
+int gbx_basis_create(gbx_basis** out, int n_shells, const int* angmom, const int* nprim,
+                     const double* center, const double* exps, const double* coefs,
+                     const int* nout, const int* sph, const int8_t* pos, const double* scl,
+                     int device);
+int gbx_basis_destroy(gbx_basis* b);
+/* Original (generalized-contraction) shell of each segmented shell: Schwarz bounds of a
+ * quartet use the bound of the original shell pairs, as gbasis screens whole generalized
+ * shells.  Default: every segmented shell is its own group. */
+int gbx_basis_set_groups(gbx_basis* b, const int* group);
+/* Number of output basis functions N (the tensor is N^4). */
+int gbx_basis_nbf(const gbx_basis* b, int64_t* nbf);
+/* Unique shell quartets and device bytes the compact store of a full call needs. */
+int gbx_basis_stats(const gbx_basis* b, int64_t* n_quartets, int64_t* compact_bytes);
+
+/*
+ * Full N^4 float64 tensor into device memory `out` (N^4 doubles, C order).  notation
+ * GBX_CHEMIST writes (ab|cd) at out[a,b,c,d]; GBX_PHYSICIST writes <ac|bd> contiguously,
+ * i.e. out[a,c,b,d] = (ab|cd).  schwarz_threshold > 0 zeroes shell quartets whose bound
+ * Q_ij Q_kl is below it (bounds on blocks without norm_cont, as gbasis's improved path).
+ * stream: a cudaStream_t (NULL = legacy default stream).  Asynchronous.
+ */
+int gbx_eri_full(gbx_basis* b, int notation, double schwarz_threshold, double* out,
+                 void* stream);
+/* Same, into host memory (page-locked or pageable); synchronous. */
+int gbx_eri_full_host(gbx_basis* b, int notation, double schwarz_threshold, double* out_host,
+                      void* stream);
+
+/* Schwarz bounds Q_p = sqrt(max |(pp|pp)|) per shell pair of the basis, host array of
+ * n_shells*n_shells doubles (symmetric). */
+int gbx_schwarz_bounds(gbx_basis* b, double* q_host);
+
+/* 4-index transform: out[i,j,k,l] = sum T[i,a] T[j,b] T[k,c] T[l,d] in[a,b,c,d] on the
+ * device (four cuBLAS DGEMMs).  in: N^4, T: n_orb x N (row-major), out: n_orb^4,
+ * work: 2 * max(N, n_orb)^4 doubles. */
+int gbx_lincomb(const double* in, int64_t n, const double* transform, int64_t n_orb,
+                double* out, double* work, void* stream);
+
+/* Coulomb matrix J[a,b] = sum_cd (ab|cd) D[c,d] from the screened unique quartets
+ * (full tensor never stored).  D, J: device N x N row-major (D symmetric). */
+int gbx_eri_coulomb_j(gbx_basis* b, const double* D, double schwarz_threshold, double* J,
+                      void* stream);
+
+/* Device-side counters of the last call on this basis: quartets computed and screened. */
+int gbx_last_counts(const gbx_basis* b, int64_t* computed, int64_t* screened);
+
+/* Phase timing: when on, full-tensor calls record CUDA events on their stream around the
+ * work-list build, the class kernels and the expansion; gbx_phase_times waits for the last
+ * call and returns the three durations in milliseconds. */
+int gbx_set_profiling(gbx_basis* b, int on);
+int gbx_phase_times(gbx_basis* b, double* ms3);
+
+/* Copy of the last error message on this thread (NUL-terminated, truncated to len). */
+int gbx_last_error(char* buf, size_t len);
+
+/* Sustained FP64 FMA rate of the device (TFLOP/s) from a dependent-FMA microbenchmark. */
+int gbx_fp64_peak(int device, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GBX_ERI_H */

@@ -340,6 +340,8 @@ def construct_array_contraction(sa, sb, sc, sd, reorder=False):
     """
     if not reorder:
         return np.transpose(quartet_cartesian(sa, sb, sc, sd), (4, 0, 5, 1, 6, 2, 7, 3))
+    if reorder == "exponent":
+        return _exponent_oriented(sa, sb, sc, sd)
     bra_sw = sa.angmom < sb.angmom
     if bra_sw:
         sa, sb = sb, sa
@@ -356,6 +358,35 @@ def construct_array_contraction(sa, sb, sc, sd, reorder=False):
         x = np.swapaxes(np.swapaxes(x, 2, 3), 6, 7)
     if bra_sw:
         x = np.swapaxes(np.swapaxes(x, 0, 1), 4, 5)
+    return np.transpose(x, (4, 0, 5, 1, 6, 2, 7, 3))
+
+
+def _pair_key(a, b):
+    return (a + b, max(a, b), a)
+
+
+def _exponent_oriented(sa, sb, sc, sd):
+    """Same integrals with the recursions run from the shell of larger maximum exponent of
+    each pair and the bra being the pair of larger (l_a + l_b, max l, l_a) — the recursion
+    order of the B200 engine (``gbasis_b200/csrc/runtime.cu``)."""
+    def tight_first(x, y):
+        ex, ey = float(np.max(x.exps)), float(np.max(y.exps))
+        return (ey > ex) or (ey == ex and y.angmom > x.angmom)
+
+    perm = [0, 1, 2, 3]
+    s = [sa, sb, sc, sd]
+    if tight_first(s[0], s[1]):
+        s[0], s[1] = s[1], s[0]
+        perm[0], perm[1] = perm[1], perm[0]
+    if tight_first(s[2], s[3]):
+        s[2], s[3] = s[3], s[2]
+        perm[2], perm[3] = perm[3], perm[2]
+    if _pair_key(s[2].angmom, s[3].angmom) > _pair_key(s[0].angmom, s[1].angmom):
+        s = s[2:] + s[:2]
+        perm = perm[2:] + perm[:2]
+    x = quartet_cartesian(*s)  # axes in the order of s
+    inv = list(np.argsort(perm))
+    x = np.transpose(x, inv + [4 + v for v in inv])
     return np.transpose(x, (4, 0, 5, 1, 6, 2, 7, 3))
 
 

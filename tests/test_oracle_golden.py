@@ -81,6 +81,10 @@ def test_quartet_blocks_all_classes():
         tol = max(ATOL, 4 * float(np.max(np.abs(imp - tru))))
         assert np.max(np.abs(reord - tru)) <= tol, [s.angmom for s in sh]
         assert np.max(np.abs(reord - imp)) <= 2 * tol, [s.angmom for s in sh]
+        # the engine's recursion order (tighter shell first, bra by angular momentum) is
+        # accurate to 1e-12 against the 40-digit values on every fixture quartet
+        expo = orc.construct_array_contraction(*sh, reorder="exponent").ravel()
+        assert np.max(np.abs(expo - tru)) <= ATOL, [s.angmom for s in sh]
 
 
 def test_horton_bec_sto6g():
