@@ -26,7 +26,7 @@ EXPORTED_SYMBOLS = (
     "gbx_basis_create", "gbx_basis_destroy", "gbx_basis_nbf", "gbx_basis_stats",
     "gbx_basis_set_groups", "gbx_eri_full", "gbx_eri_full_host", "gbx_schwarz_bounds",
     "gbx_lincomb", "gbx_eri_coulomb_j", "gbx_last_counts", "gbx_last_error", "gbx_fp64_peak",
-    "gbx_set_profiling", "gbx_phase_times",
+    "gbx_set_profiling", "gbx_phase_times", "gbx_eri_full_noalloc",
 )
 
 
@@ -73,6 +73,7 @@ def lib():
             "gbx_fp64_peak": [_I, ctypes.POINTER(_D)],
             "gbx_set_profiling": [_P, _I],
             "gbx_phase_times": [_P, _P],
+            "gbx_eri_full_noalloc": [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
         }
         for name, args in sig.items():
             f = getattr(L, name)

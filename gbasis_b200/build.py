@@ -40,11 +40,11 @@ def sources(lmax):
     import gen_eri  # noqa: E402
     gen = gen_eri.emit_sources(GEN, lmax)
     return [os.path.join(GEN, g) for g in gen] + [
-        os.path.join(CSRC, f) for f in ("runtime.cu", "pipeline.cu", "extras.cu")]
+        os.path.join(CSRC, f) for f in ("runtime.cu", "pipeline.cu", "extras.cu", "noalloc.cu")]
 
 
 KERNEL_DEPS = ("gbx_common.cuh", "eri_kernels.cuh", "errors.h", "_gen/eri_gen.cuh")
-HOST_DEPS = ("gbx_common.cuh", "runtime.h", "errors.h")
+HOST_DEPS = ("gbx_common.cuh", "runtime.h", "errors.h", "pipeline_kernels.cuh")
 
 
 def _deps_mtime(src):

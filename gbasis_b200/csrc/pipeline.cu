@@ -12,6 +12,7 @@
 
 #include "gbx_eri.h"
 #include "gbx_common.cuh"
+#include "pipeline_kernels.cuh"
 #include "runtime.h"
 
 namespace gbx {
@@ -62,12 +63,6 @@ __global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,
 }
 
 // ------------------------------------------------------------------- K2
-struct BuildBlock {
-  int pb0, nb, pk0, nk;
-  int tri, blk;
-  long long work_off, ncand;
-};
-
 __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* __restrict__ bb,
                            const double* __restrict__ qs, double tau, int2* __restrict__ work,
                            int* __restrict__ counts) {
@@ -103,18 +98,6 @@ __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* _
 }
 
 // ------------------------------------------------------------------- K6
-struct ExpandArgs {
-  long long n;
-  int nsh, notation;
-  const int* fsh;
-  const int* fcomp;
-  const int* pair_of;
-  const int4* pinfo;  // (cls, local, fo, nB)
-  const BlockDev* blocks;
-  const double* compact;
-  double* out;
-};
-
 __device__ __forceinline__ long long pair_row(const ExpandArgs& e, int s1, int c1, int s2, int c2,
                                               int4& info) {
   const int pe = e.pair_of[s1 * e.nsh + s2];

@@ -1,0 +1,36 @@
+// Argument structs and declarations of the pipeline kernels defined in pipeline.cu.
+#pragma once
+#include "gbx_common.cuh"
+
+namespace gbx {
+
+// One class block of the work-list build (K2).
+struct BuildBlock {
+  int pb0, nb, pk0, nk;
+  int tri, blk;
+  long long work_off, ncand;
+};
+
+// Full-tensor expansion (K6).
+struct ExpandArgs {
+  long long n;
+  int nsh, notation;
+  const int* fsh;
+  const int* fcomp;
+  const int* pair_of;
+  const int4* pinfo;  // (cls, local, fo, nB)
+  const BlockDev* blocks;
+  const double* compact;
+  double* out;
+};
+
+__global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,
+                                const ShellDev* __restrict__ shells,
+                                const double* __restrict__ exps, const double* __restrict__ coefs,
+                                PrimPair* __restrict__ prims);
+__global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* __restrict__ bb,
+                           const double* __restrict__ qs, double tau, int2* __restrict__ work,
+                           int* __restrict__ counts);
+__global__ void expand_full(const ExpandArgs e);
+
+}  // namespace gbx

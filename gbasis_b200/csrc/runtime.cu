@@ -59,17 +59,21 @@ static long double boys_series(int m, long double T) {
 static std::mutex g_boys_mu;
 static double* g_boys_dev[64] = {nullptr};
 
+void boys_host_table(double* h) {
+  for (int n = 0; n < kBoysNGrid; ++n) {
+    const long double T = (long double)n / 10.0L;
+    for (int m = 0; m < kBoysOrders; ++m)
+      h[(size_t)n * (kBoysOrders + 1) + m] = (double)boys_series(m, T);
+    h[(size_t)n * (kBoysOrders + 1) + kBoysOrders] = (double)expl(-T);
+  }
+}
+
 int boys_table(int device, const double** out) {
   std::lock_guard<std::mutex> lk(g_boys_mu);
   if (device < 0 || device >= 64) return set_error(GBX_ERR_INVALID, "bad device %d", device);
   if (!g_boys_dev[device]) {
     std::vector<double> h((size_t)kBoysNGrid * (kBoysOrders + 1));
-    for (int n = 0; n < kBoysNGrid; ++n) {
-      const long double T = (long double)n / 10.0L;
-      for (int m = 0; m < kBoysOrders; ++m)
-        h[(size_t)n * (kBoysOrders + 1) + m] = (double)boys_series(m, T);
-      h[(size_t)n * (kBoysOrders + 1) + kBoysOrders] = (double)expl(-T);
-    }
+    boys_host_table(h.data());
     double* d = nullptr;
     GBX_CUDA(cudaMalloc(&d, h.size() * sizeof(double)), "cudaMalloc(boys table)");
     GBX_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice),
@@ -127,7 +131,7 @@ int Basis::ensure_scratch(size_t compact_elems, size_t work_elems) {
   return GBX_OK;
 }
 
-static int build_basis(Basis& B, int n, const int* angmom, const int* nprim, const double* center,
+int build_basis(Basis& B, int n, const int* angmom, const int* nprim, const double* center,
                        const double* exps, const double* coefs, const int* nout, const int* sph,
                        const int8_t* pos, const double* scl) {
   B.shells.resize(n);

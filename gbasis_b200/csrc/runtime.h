@@ -71,6 +71,10 @@ struct Basis {
   int ensure_scratch(size_t compact_elems, size_t work_elems);
 };
 
+int build_basis(Basis& B, int n, const int* angmom, const int* nprim, const double* center,
+                const double* exps, const double* coefs, const int* nout, const int* sph,
+                const int8_t* pos, const double* scl);
+void boys_host_table(double* h);
 int upload_basis(Basis& B);
 int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st);
 int run_compact(Basis& B, double tau, cudaStream_t st);

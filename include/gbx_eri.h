@@ -100,6 +100,23 @@ int gbx_schwarz_bounds(gbx_basis* b, double* q_host);
 int gbx_lincomb(const double* in, int64_t n, const double* transform, int64_t n_orb,
                 double* out, double* work, void* stream);
 
+/*
+ * Allocation-free full tensor (no counterpart in the reference: gbasis has no device code).
+ * For callers that cannot call cudaMalloc while they run this library — e.g. a process
+ * whose device memory is owned by another allocator that reserved most of the GPU up
+ * front, or a pipeline that cannot take the device-wide synchronisation of cudaFree.  Same
+ * basis arrays as gbx_basis_create (no handle), same output as gbx_eri_full (device `out`,
+ * N^4 doubles, caller-owned), no Schwarz screening.  Every intermediate lives in one static
+ * device array of 64 MiB that each GPU loading the library holds until exit; bases needing
+ * more are rejected with GBX_ERR_INVALID.  The first call on a device resolves that array's
+ * address (cudaGetSymbolAddress) — make it before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the caller.
+ */
+int gbx_eri_full_noalloc(int n_shells, const int* angmom, const int* nprim,
+                         const double* center, const double* exps, const double* coefs,
+                         const int* nout, const int* sph, const int8_t* pos, const double* scl,
+                         int notation, double* out, void* stream);
+
 /* Coulomb matrix J[a,b] = sum_cd (ab|cd) D[c,d] from the screened unique quartets
  * (full tensor never stored).  D, J: device N x N row-major (D symmetric). */
 int gbx_eri_coulomb_j(gbx_basis* b, const double* D, double schwarz_threshold, double* J,
