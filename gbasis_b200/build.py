@@ -21,7 +21,7 @@ GEN = os.path.join(CSRC, "_gen")
 BUILD = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libgbx_eri.so")
-LMAX_DEFAULT = 2
+LMAX_DEFAULT = 3
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
@@ -40,11 +40,13 @@ def sources(lmax):
     import gen_eri  # noqa: E402
     gen = gen_eri.emit_sources(GEN, lmax)
     return [os.path.join(GEN, g) for g in gen] + [
-        os.path.join(CSRC, f) for f in ("runtime.cu", "pipeline.cu", "extras.cu", "noalloc.cu")]
+        os.path.join(CSRC, f) for f in ("runtime.cu", "pipeline.cu", "extras.cu", "noalloc.cu",
+                                        "coop_kernel.cu")]
 
 
 KERNEL_DEPS = ("gbx_common.cuh", "eri_kernels.cuh", "errors.h", "_gen/eri_gen.cuh")
-HOST_DEPS = ("gbx_common.cuh", "runtime.h", "errors.h", "pipeline_kernels.cuh")
+HOST_DEPS = ("gbx_common.cuh", "runtime.h", "errors.h", "pipeline_kernels.cuh", "coop.cuh",
+             "_gen/coop_programs.cuh")
 
 
 def _deps_mtime(src):

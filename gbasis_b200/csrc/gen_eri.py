@@ -325,7 +325,20 @@ def emit_sph_and_norms(w, lmax):
         w("}")
 
 
-def emit_all(lmax):
+LIGHT_LIMIT = 170  # doubles of [e0|f0] + (ab|cd) one thread may hold
+
+
+def is_light(c):
+    """Classes evaluated by one thread in registers; the rest run on the cooperative kernel."""
+    la, lb, lc, ld = c
+    ne = sum(ncart(e) for e in range(la, la + lb + 1))
+    nf = sum(ncart(f) for f in range(lc, lc + ld + 1))
+    return ne * nf + ncart(la) * ncart(lb) * ncart(lc) * ncart(ld) <= LIGHT_LIMIT
+
+
+def emit_all(lmax, classes=None):
+    if classes is None:
+        classes = [c for c in canonical_classes(lmax) if is_light(c)]
     lines = []
     w = lines.append
     w("// Generated by gen_eri.py — class-specialised ERI recursions. Do not edit by hand.")
@@ -334,7 +347,7 @@ def emit_all(lmax):
     w("namespace gbx { namespace gen {")
     emit_sph_and_norms(w, lmax)
     w("template <int LA, int LB, int LC, int LD> struct Cls;")
-    for la, lb, lc, ld in canonical_classes(lmax):
+    for la, lb, lc, ld in classes:
         g = best_prim(la, lb, lc, ld)
         h = HrrGen(la, lb, lc, ld)
         NE, NF = len(g.E), len(g.F)
@@ -368,8 +381,10 @@ def emit_all(lmax):
 
 
 def emit_sources(outdir, lmax):
-    """Write eri_gen.cuh, one instantiation file per bra l_a and the class dispatch."""
+    """Write eri_gen.cuh (light classes), their instantiation files, the cooperative programs
+    of the heavy classes (coop_programs.cuh) and the class dispatch."""
     import os
+    import gen_coop
     os.makedirs(outdir, exist_ok=True)
 
     def put(name, text):
@@ -378,20 +393,23 @@ def emit_sources(outdir, lmax):
             with open(path, "w") as f:
                 f.write(text)
 
-    put("eri_gen.cuh", emit_all(lmax))
-    classes = canonical_classes(lmax)
+    every = canonical_classes(lmax)
+    light = [c for c in every if is_light(c)]
+    heavy = [c for c in every if not is_light(c)]
+    put("eri_gen.cuh", emit_all(lmax, light))
+    gen_coop.emit(heavy, os.path.join(outdir, "coop_programs.cuh"))
     files = []
-    # spread the classes over translation units of similar compile cost (code size)
-    nbins = 16
+    # spread the light classes over translation units of similar compile cost (code size)
+    nbins = 12
     bins = [[] for _ in range(nbins)]
     load = [0] * nbins
     cost = {c: best_prim(*c).op_count() + 4 * ncart(c[0]) * ncart(c[1]) * ncart(c[2]) * ncart(c[3])
-            for c in classes}
-    for c in sorted(classes, key=lambda c: -cost[c]):
+            for c in light}
+    for c in sorted(light, key=lambda c: -cost[c]):
         k = load.index(min(load))
         bins[k].append(c)
         load[k] += cost[c]
-    for la, mine in enumerate(b for b in bins if b):
+    for k, mine in enumerate(b for b in bins if b):
         lines = ["// Generated by gen_eri.py: explicit instantiations of the class kernels.",
                  '#include "../eri_kernels.cuh"',
                  '#include "../errors.h"',
@@ -405,24 +423,28 @@ def emit_sources(outdir, lmax):
             lines.append(f"template int launch_t<{c[0]}, {c[1]}, {c[2]}, {c[3]}>(const EriLaunch&, "
                          "int, cudaStream_t);")
         lines.append("}  // namespace gbx")
-        name = f"eri_cls_l{la}.cu"
+        name = f"eri_cls_{k:02d}.cu"
         put(name, "\n".join(lines) + "\n")
         files.append(name)
     lines = ["// Generated by gen_eri.py: (la,lb,lc,ld) -> class kernel launcher.",
+             '#include "../coop.cuh"',
              '#include "../runtime.h"',
              "namespace gbx {",
              "template <int LA, int LB, int LC, int LD>",
              "int launch_t(const EriLaunch& a, int grid, cudaStream_t st);"]
-    for c in classes:
+    for c in light:
         lines.append(f"extern template int launch_t<{c[0]}, {c[1]}, {c[2]}, {c[3]}>(const EriLaunch&, "
                      "int, cudaStream_t);")
     lines.append(f"int compiled_lmax() {{ return {lmax}; }}")
     lines.append("int launch_class(int la, int lb, int lc, int ld, const EriLaunch& a, int grid, "
                  "cudaStream_t st) {")
     lines.append("  switch (((la * 8 + lb) * 8 + lc) * 8 + ld) {")
-    for c in classes:
+    for c in light:
         key = ((c[0] * 8 + c[1]) * 8 + c[2]) * 8 + c[3]
         lines.append(f"    case {key}: return launch_t<{c[0]}, {c[1]}, {c[2]}, {c[3]}>(a, grid, st);")
+    for j, c in enumerate(heavy):
+        key = ((c[0] * 8 + c[1]) * 8 + c[2]) * 8 + c[3]
+        lines.append(f"    case {key}: return launch_coop({j}, a, st);")
     lines.append("    default: break;")
     lines.append("  }")
     lines.append('  return set_error(GBX_ERR_UNSUPPORTED, "no kernel for class (%d %d|%d %d)", '

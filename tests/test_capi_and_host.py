@@ -127,3 +127,75 @@ def test_generated_recursions_match_oracle(cls):
     cn = [1 / np.sqrt(np.prod(orc.factorial2(2 * orc.cart_components(l) - 1), axis=1)) for l in cls]
     got = np.einsum("abcd,a,b,c,d->abcd", got, *cn)
     np.testing.assert_allclose(got, ref, rtol=1e-11, atol=1e-14)
+
+
+import gen_coop  # noqa: E402
+
+
+def _run_coop_program(cls, shells):
+    """Interpret one class's cooperative program (as the warp kernel does) for one primitive
+    quartet, Cartesian output (component norms applied)."""
+    prog = gen_coop.program(*cls)
+    (a, A), (b, B), (c, C), (d, D) = [(float(s.exps[0]), s.coord) for s in shells]
+    z, e = a + b, c + d
+    P, Q = (a * A + b * B) / z, (c * C + d * D) / e
+    rho = z * e / (z + e)
+    PQ = P - Q
+    T = rho * PQ @ PQ
+    norm = np.prod([(2 * s.exps[0] / np.pi) ** 0.75 * (4 * s.exps[0]) ** (s.angmom / 2)
+                    for s in shells])
+    pref = 2 * np.pi ** 2.5 / (z * e * np.sqrt(z + e)) * np.exp(-a * b / z * (A - B) @ (A - B)) \
+        * np.exp(-c * d / e * (C - D) @ (C - D)) * norm
+    L = sum(cls)
+    X = np.zeros(prog["nX"])
+    X[:L + 1] = [pref * float(orc.boys(m, T)) for m in range(L + 1)]
+    PA, QC = P - A, Q - C
+    rz, ze = rho / z, z / e
+    WP, CE = -rz * PQ, QC + ze * PA
+    for (dst, s1, s2, s3, s4, i, k, _) in prog["vins"]:
+        v = PA[i] * X[s1] + WP[i] * X[s2]
+        if k:
+            v += k * 0.5 / z * (X[s3] - rz * X[s4])
+        X[dst] = v
+    for (dst, s1, s2, s3, s4, i, k1, k2) in prog["tins"]:
+        v = CE[i] * X[s1] - ze * X[s2]
+        if k1:
+            v += k1 * 0.5 / e * X[s3]
+        if k2:
+            v += k2 * 0.5 / e * X[s4]
+        X[dst] = v
+    NE, NF = prog["NE"], prog["NF"]
+    acc = X[prog["targets"]].reshape(NE, NF)
+    CD, AB = C - D, A - B
+    NCD = len(prog["kfin"])
+    HF = np.zeros((NE, NCD))
+    for r in range(NE):
+        K = np.zeros(prog["nK"])
+        K[:NF] = acc[r]
+        for (dst, s1, s2, _, _, i, _, _) in prog["kins"]:
+            K[dst] = K[s1] + CD[i] * K[s2]
+        HF[r] = K[prog["kfin"]]
+    NAB = len(prog["bfin"])
+    out = np.zeros((NAB, NCD))
+    for col in range(NCD):
+        Bn = np.zeros(prog["nB"])
+        Bn[:NE] = HF[:, col]
+        for (dst, s1, s2, _, _, i, _, _) in prog["bins"]:
+            Bn[dst] = Bn[s1] + AB[i] * Bn[s2]
+        out[:, col] = Bn[prog["bfin"]]
+    la, lb, lc, ld = cls
+    cn = [1 / np.sqrt(np.prod(orc.factorial2(2 * orc.cart_components(l) - 1), axis=1)) for l in cls]
+    out = out.reshape(len(cn[0]), len(cn[1]), len(cn[2]), len(cn[3]))
+    return np.einsum("abcd,a,b,c,d->abcd", out, *cn)
+
+
+@pytest.mark.parametrize("cls", [(2, 2, 2, 2), (2, 2, 1, 2), (1, 2, 1, 2), (3, 3, 3, 3),
+                                 (3, 0, 2, 2), (0, 3, 3, 1), (3, 2, 2, 3)])
+def test_cooperative_programs_match_oracle(cls):
+    rng = np.random.default_rng(7 + sum(cls))
+    shells = [GeneralizedContractionShell(l, rng.uniform(-1, 1, 3), np.array([1.0]),
+                                          np.array([rng.uniform(0.4, 2.5)]), "cartesian")
+              for l in cls]
+    ref = orc.quartet_cartesian(*shells)[..., 0, 0, 0, 0]
+    got = _run_coop_program(cls, shells)
+    np.testing.assert_allclose(got, ref, rtol=1e-10, atol=1e-13)
