@@ -27,6 +27,7 @@ EXPORTED_SYMBOLS = (
     "gbx_basis_set_groups", "gbx_eri_full", "gbx_eri_full_host", "gbx_schwarz_bounds",
     "gbx_lincomb", "gbx_eri_coulomb_j", "gbx_last_counts", "gbx_last_error", "gbx_fp64_peak",
     "gbx_set_profiling", "gbx_phase_times", "gbx_eri_full_noalloc",
+    "gbx_num_blocks", "gbx_block_info", "gbx_set_team", "gbx_block_times",
 )
 
 
@@ -74,6 +75,11 @@ def lib():
             "gbx_set_profiling": [_P, _I],
             "gbx_phase_times": [_P, _P],
             "gbx_eri_full_noalloc": [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
+            "gbx_num_blocks": [_P, ctypes.POINTER(_I)],
+            "gbx_block_info": [_P, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(_D),
+                               ctypes.POINTER(_I64)],
+            "gbx_set_team": [_P, _I, _I],
+            "gbx_block_times": [_P, _P, _I],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -216,7 +222,7 @@ def _ptr(a):
 class DeviceBasis:
     """A basis resident on one CUDA device (owns a ``gbx_basis`` handle)."""
 
-    def __init__(self, shells, coord_types=None, raw=False, device=None):
+    def __init__(self, shells, coord_types=None, raw=False, device=None, tuned=True):
         L = lib()
         if device is None:
             device = _current_device()
@@ -233,6 +239,9 @@ class DeviceBasis:
         n = ctypes.c_int64()
         check(L.gbx_basis_nbf(h, ctypes.byref(n)))
         self.nbf = int(n.value)
+        if tuned:
+            from .autotune import apply_cache
+            apply_cache(self)
 
     def stats(self):
         q, b = ctypes.c_int64(), ctypes.c_int64()
@@ -260,13 +269,37 @@ class DeviceBasis:
         check(lib().gbx_schwarz_bounds(self.handle, _ptr(q)), "gbx_schwarz_bounds")
         return q
 
-    def set_profiling(self, on=True):
-        check(lib().gbx_set_profiling(self.handle, int(bool(on))), "gbx_set_profiling")
+    def set_profiling(self, level=1):
+        """0 off; 1 phase events; 2 phase and per-block events (blocks run one at a time)."""
+        check(lib().gbx_set_profiling(self.handle, int(level)), "gbx_set_profiling")
 
     def phase_times(self):
         """(work-list build, class kernels, expansion) of the last call, milliseconds."""
         ms = np.zeros(3)
         check(lib().gbx_phase_times(self.handle, _ptr(ms)), "gbx_phase_times")
+        return ms
+
+    def blocks(self):
+        """[(class (la, lb, lc, ld), team, mean primitive quartets, quartets)] per class block."""
+        n = ctypes.c_int()
+        check(lib().gbx_num_blocks(self.handle, ctypes.byref(n)))
+        out = []
+        for k in range(n.value):
+            c4 = np.zeros(4, dtype=np.int32)
+            t, ap, nq = ctypes.c_int(), ctypes.c_double(), ctypes.c_int64()
+            check(lib().gbx_block_info(self.handle, k, _ptr(c4), ctypes.byref(t), ctypes.byref(ap),
+                                       ctypes.byref(nq)))
+            out.append((tuple(int(v) for v in c4), t.value, ap.value, nq.value))
+        return out
+
+    def set_team(self, k, team):
+        check(lib().gbx_set_team(self.handle, int(k), int(team)), "gbx_set_team")
+
+    def block_times(self):
+        n = ctypes.c_int()
+        check(lib().gbx_num_blocks(self.handle, ctypes.byref(n)))
+        ms = np.zeros(n.value)
+        check(lib().gbx_block_times(self.handle, _ptr(ms), n.value), "gbx_block_times")
         return ms
 
     def last_counts(self):

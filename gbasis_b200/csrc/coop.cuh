@@ -9,6 +9,7 @@ struct CoopMeta {
   int la, lb, lc, ld, L, NE, NF, nX, nK, nB;
   int v_ins, v_lv, v_nlv, t_ins, t_lv, t_nlv, k_ins, k_lv, k_nlv, b_ins, b_lv, b_nlv;
   int targets, kfin, bfin;
+  int n_ins, n_idx;  // instructions (VRR, ETR, ket, bra programs, contiguous) and indices
 };
 
 // Find the program of class (la, lb | lc, ld); -1 when the class is not cooperative.

@@ -26,6 +26,7 @@ struct CoopArgs {
   EriLaunch a;
   CoopMeta m;
   int R, Cc, smem_per_warp;  // rows / columns per HRR chunk, doubles of smem per warp
+  int prog_doubles;          // shared memory taken by the staged programs (0: read globally)
 };
 
 __device__ __forceinline__ double pick3(int d, double x, double y, double z) {
@@ -76,13 +77,58 @@ __device__ void boys_to_smem(int L, double T, double pref, const double* __restr
   }
 }
 
+// Lane m <= L writes pref * F_m(T) to X[m]: T < 40 by the 8-term Taylor expansion of F_m
+// around the nearest grid point (orders m..m+7 of the table), T >= 40 by F_0 = sqrt(pi/T)/2
+// and m upward steps F_{k+1} = ((2k+1) F_k - e^{-T})/(2T).
+__device__ __forceinline__ void boys_lanes(int L, int lane, double T, double pref,
+                                           const double* __restrict__ tab, double* X) {
+  if (lane > L) return;
+  double f;
+  if (T < kBoysTMax) {
+    const int n = __double2int_rn(T * 10.0);
+    const double x = fma(-T, 10.0, (double)n) * 0.1;
+    const double* g = tab + n * (kBoysOrders + 1) + lane;
+    f = g[7] * (1.0 / 5040);
+    f = fma(f, x, g[6] * (1.0 / 720));
+    f = fma(f, x, g[5] * (1.0 / 120));
+    f = fma(f, x, g[4] * (1.0 / 24));
+    f = fma(f, x, g[3] * (1.0 / 6));
+    f = fma(f, x, g[2] * 0.5);
+    f = fma(f, x, g[1]);
+    f = fma(f, x, g[0]);
+  } else {
+    const double r = rsqrt(T);
+    f = 0.88622692545275801365 * r;
+    if (lane > 0) {
+      const double emT = exp(-T), o2T = 0.5 * r * r;
+      for (int m = 0; m < lane; ++m) f = fma((double)(2 * m + 1), f, -emT) * o2T;
+    }
+  }
+  X[lane] = f * pref;
+}
+
 __global__ void eri_coop(const CoopArgs A) {
   extern __shared__ double smem[];
   const EriLaunch& a = A.a;
   const CoopMeta& M = A.m;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  double* S = smem + (size_t)wib * A.smem_per_warp;
+  // the class's programs, staged once per CTA when they fit (A.prog_doubles > 0)
+  short(*s_ins)[8] = reinterpret_cast<short(*)[8]>(smem);
+  short* s_idx = reinterpret_cast<short*>(smem) + 8 * M.n_ins;
+  const bool staged = A.prog_doubles > 0;
+  if (staged) {
+    const int4* src = reinterpret_cast<const int4*>(&kCoopIns[M.v_ins][0]);
+    int4* dst4 = reinterpret_cast<int4*>(smem);
+    for (int i = threadIdx.x; i < M.n_ins; i += blockDim.x) dst4[i] = src[i];
+    for (int i = threadIdx.x; i < M.n_idx; i += blockDim.x) s_idx[i] = kCoopIdx[M.targets + i];
+    __syncthreads();
+  }
+  auto INS = [&](int i) -> const short* {
+    return staged ? s_ins[i - M.v_ins] : kCoopIns[i];
+  };
+  auto IDX = [&](int j) -> int { return staged ? s_idx[j - M.targets] : kCoopIdx[j]; };
+  double* S = smem + A.prog_doubles + (size_t)wib * A.smem_per_warp;
   const int NENF = M.NE * M.NF;
   const int NCA = ncart(M.la), NCB = ncart(M.lb), NCC = ncart(M.lc), NCDD = ncart(M.ld);
   const int NCD = NCC * NCDD, NAB = NCA * NCB;
@@ -117,12 +163,12 @@ __global__ void eri_coop(const CoopArgs A) {
         const double CEx = fma(ze, bp.Xx, kp.Xx), CEy = fma(ze, bp.Xy, kp.Xy),
                      CEz = fma(ze, bp.Xz, kp.Xz);
         __syncwarp();
-        if (lane == 0) boys_to_smem(M.L, T, bp.C * kp.C * r, a.boys_tab, X);
+        boys_lanes(M.L, lane, T, bp.C * kp.C * r, a.boys_tab, X);
         __syncwarp();
         for (int l = 0; l < M.v_nlv; ++l) {
           const int b = kCoopLv[M.v_lv + l], e = kCoopLv[M.v_lv + l + 1];
           for (int i = b + lane; i < e; i += 32) {
-            const short* I = kCoopIns[M.v_ins + i];
+            const short* I = INS(M.v_ins + i);
             const int dir = I[5];
             double v = fma(pick3(dir, bp.Xx, bp.Xy, bp.Xz), X[I[1]],
                            pick3(dir, WPx, WPy, WPz) * X[I[2]]);
@@ -134,7 +180,7 @@ __global__ void eri_coop(const CoopArgs A) {
         for (int l = 0; l < M.t_nlv; ++l) {
           const int b = kCoopLv[M.t_lv + l], e = kCoopLv[M.t_lv + l + 1];
           for (int i = b + lane; i < e; i += 32) {
-            const short* I = kCoopIns[M.t_ins + i];
+            const short* I = INS(M.t_ins + i);
             const int dir = I[5];
             double v = fma(pick3(dir, CEx, CEy, CEz), X[I[1]], -ze * X[I[2]]);
             if (I[6]) v = fma(I[6] * o2e, X[I[3]], v);
@@ -143,7 +189,7 @@ __global__ void eri_coop(const CoopArgs A) {
           }
           __syncwarp();
         }
-        for (int i = lane; i < NENF; i += 32) ACC[i] += X[kCoopIdx[M.targets + i]];
+        for (int i = lane; i < NENF; i += 32) ACC[i] += X[IDX(M.targets + i)];
       }
     }
     __syncwarp();
@@ -160,7 +206,7 @@ __global__ void eri_coop(const CoopArgs A) {
         const int b = kCoopLv[M.k_lv + l], e = kCoopLv[M.k_lv + l + 1], cnt = e - b;
         for (int i = lane; i < rr * cnt; i += 32) {
           const int r = i / cnt;
-          const short* I = kCoopIns[M.k_ins + b + (i - r * cnt)];
+          const short* I = INS(M.k_ins + b + (i - r * cnt));
           double* Kr = KN + r * M.nK;
           Kr[I[0]] = fma(pick3(I[5], Q.ABx, Q.ABy, Q.ABz), Kr[I[2]], Kr[I[1]]);
         }
@@ -168,7 +214,7 @@ __global__ void eri_coop(const CoopArgs A) {
       }
       for (int i = lane; i < rr * NCD; i += 32) {
         const int r = i / NCD, j = i - r * NCD;
-        HF[(r0 + r) * NCD + j] = KN[r * M.nK + kCoopIdx[M.kfin + j]];
+        HF[(r0 + r) * NCD + j] = KN[r * M.nK + IDX(M.kfin + j)];
       }
       __syncwarp();
     }
@@ -229,7 +275,7 @@ __global__ void eri_coop(const CoopArgs A) {
         const int b = kCoopLv[M.b_lv + l], e = kCoopLv[M.b_lv + l + 1], cnt = e - b;
         for (int i = lane; i < cc * cnt; i += 32) {
           const int c = i / cnt;
-          const short* I = kCoopIns[M.b_ins + b + (i - c * cnt)];
+          const short* I = INS(M.b_ins + b + (i - c * cnt));
           double* Bc = BN + c * M.nB;
           Bc[I[0]] = fma(pick3(I[5], P.ABx, P.ABy, P.ABz), Bc[I[2]], Bc[I[1]]);
         }
@@ -237,7 +283,7 @@ __global__ void eri_coop(const CoopArgs A) {
       }
       for (int i = lane; i < cc * NAB; i += 32) {
         const int c = i / NAB, j = i - c * NAB;
-        OB[i] = BN[c * M.nB + kCoopIdx[M.bfin + j]];
+        OB[i] = BN[c * M.nB + IDX(M.bfin + j)];
       }
       __syncwarp();
       // axis B then A (per column), result in OB as [c][ua][ub] with row stride nBi
@@ -322,8 +368,13 @@ int launch_coop(int prog, const EriLaunch& a, cudaStream_t st) {
   const long long per_warp = size_for(R, Cc);
   A.smem_per_warp = (int)per_warp;
   const long long max_smem = 227 * 1024;
-  int wpc = (int)std::max<long long>(1, std::min<long long>(4, max_smem / (per_warp * 8)));
-  const size_t smem = (size_t)wpc * per_warp * 8;
+  const long long prog_bytes = (long long)M.n_ins * 16 + (long long)M.n_idx * 2;
+  A.prog_doubles = 0;
+  if (prog_bytes <= 32 * 1024 && prog_bytes + per_warp * 8 <= max_smem)
+    A.prog_doubles = (int)((prog_bytes + 15) / 16 * 2);
+  const long long avail = max_smem - (long long)A.prog_doubles * 8;
+  int wpc = (int)std::max<long long>(1, std::min<long long>(4, avail / (per_warp * 8)));
+  const size_t smem = (size_t)A.prog_doubles * 8 + (size_t)wpc * per_warp * 8;
   if ((long long)smem > max_smem)
     return set_error(GBX_ERR_UNSUPPORTED, "class (%d%d|%d%d) needs %zu bytes of shared memory",
                      M.la, M.lb, M.lc, M.ld, smem);

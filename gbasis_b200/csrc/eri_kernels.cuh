@@ -109,20 +109,33 @@ __global__ void __launch_bounds__(kEriThreads) eri_block_fp64(const EriLaunch a)
   stage_boys<L>(a.boys_tab, s_tab, s_exp);
   __syncthreads();
 
+  // A team of `team` consecutive lanes (1..32, power of two) shares one quartet: its lanes
+  // take interleaved primitive quartets and the accumulators are summed with shuffles.  The
+  // loop is warp-uniform (each warp takes 32/team quartets per step) so that the shuffles
+  // always see the whole warp.
   const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < count; w += stride) {
-    const int2 pq = a.work[a.work_off + w];
+  const int team = a.team > 0 ? a.team : 1;
+  const int lane = threadIdx.x & 31;
+  const int tl = lane & (team - 1);
+  const int per_warp = 32 / team;
+  const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long wb = gwarp * per_warp; wb < count; wb += nwarps * per_warp) {
+    const long long w = wb + lane / team;
+    const bool valid = w < count;
+    const int2 pq = valid ? a.work[a.work_off + w] : make_int2(0, 0);
     const PairDev P = a.pairs[pq.x];
     const PairDev Q = a.pairs[pq.y];
     double acc[C::NE * C::NF];
 #pragma unroll
     for (int i = 0; i < C::NE * C::NF; ++i) acc[i] = 0.0;
 
-    for (int ip = 0; ip < P.nprim; ++ip) {
-      const PrimPair bp = a.prims[P.prim_off + ip];
-      const double o2z = 0.5 * bp.izeta;
-      for (int jq = 0; jq < Q.nprim; ++jq) {
+    const int nprim = valid ? P.nprim * Q.nprim : 0;
+    int ip = tl / Q.nprim, jq = tl - ip * Q.nprim;
+    for (int idx = tl; idx < nprim; idx += team) {
+      {
+        const PrimPair bp = a.prims[P.prim_off + ip];
+        const double o2z = 0.5 * bp.izeta;
         const PrimPair kp = a.prims[Q.prim_off + jq];
         const double r = rsqrt(bp.zeta + kp.zeta);
         const double inv = r * r;
@@ -140,7 +153,17 @@ __global__ void __launch_bounds__(kEriThreads) eri_block_fp64(const EriLaunch a)
                                  rz, fma(ze, bp.Xx, kp.Xx), fma(ze, bp.Xy, kp.Xy),
                                  fma(ze, bp.Xz, kp.Xz), ze, o2e, acc);
       }
+      jq += team;
+      while (jq >= Q.nprim) {
+        jq -= Q.nprim;
+        ++ip;
+      }
     }
+    for (int o = team >> 1; o > 0; o >>= 1) {
+#pragma unroll
+      for (int i = 0; i < C::NE * C::NF; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+    }
+    if (!valid || tl != 0) continue;
 
     double out[C::NAB * C::NCD];
     C::hrr(acc, P.ABx, P.ABy, P.ABz, Q.ABx, Q.ABy, Q.ABz, out);

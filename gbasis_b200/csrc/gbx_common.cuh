@@ -80,6 +80,7 @@ struct EriLaunch {
   double* out;              // compact store
   long long base, ncols;
   int mode;                 // 0 = write block, 1 = Schwarz diagonal (max |.| -> qout)
+  int team;                 // lanes per quartet in the register kernel (1..32, power of two)
   double* qout;             // per-pair Schwarz value (mode 1)
   int* status;              // device error flag
 };

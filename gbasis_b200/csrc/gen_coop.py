@@ -151,6 +151,8 @@ def emit(classes, path):
         for key in ("targets", "kfin", "bfin"):
             m[key] = len(idx)
             idx += p[key]
+        m["n_ins"] = len(ins) - m["v_ins"]
+        m["n_idx"] = len(idx) - m["targets"]
         metas.append(m)
     import math
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
@@ -177,11 +179,11 @@ def emit(classes, path):
         la, lb, lc, ld = m["cls"]
         lines.append(
             "  {%d, %d, %d, %d, %d, %d, %d, %d, %d, %d, "
-            "%d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d}," % (
+            "%d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d}," % (
                 la, lb, lc, ld, m["L"], m["NE"], m["NF"], m["nX"], m["nK"], m["nB"],
                 m["v_ins"], m["v_lv"], m["v_nlv"], m["t_ins"], m["t_lv"], m["t_nlv"],
                 m["k_ins"], m["k_lv"], m["k_nlv"], m["b_ins"], m["b_lv"], m["b_nlv"],
-                m["targets"], m["kfin"], m["bfin"]))
+                m["targets"], m["kfin"], m["bfin"], m["n_ins"], m["n_idx"]))
     lines.append("};")
     lines.append("}  // namespace gbx")
     text = "\n".join(lines) + "\n"

@@ -121,6 +121,7 @@ extern "C" int gbx_eri_full_noalloc(int n_shells, const int* angmom, const int* 
   const size_t o_cmap = cv.take(cmap.size() * sizeof(int2));
   const size_t o_pinfo = cv.take(np * sizeof(int4));
   const size_t o_counts = cv.take(nblk * sizeof(int));
+  const size_t o_ftab = cv.take(B.h_ftab.size() * sizeof(long long));
   const size_t o_work = cv.take((size_t)B.n_quartets * sizeof(int2));
   const size_t o_boys = cv.take(sizeof(g_boys_host));
   const size_t o_compact = cv.take((size_t)B.compact_elems * sizeof(double));
@@ -147,7 +148,8 @@ extern "C" int gbx_eri_full_noalloc(int n_shells, const int* angmom, const int* 
       (s = up(o_bb, bb.data(), nblk * sizeof(BuildBlock))) ||
       (s = up(o_cmap, cmap.data(), cmap.size() * sizeof(int2))) ||
       (s = up(o_pinfo, pinfo.data(), np * sizeof(int4))) ||
-      (s = up(o_boys, g_boys_host, sizeof(g_boys_host))))
+      (s = up(o_boys, g_boys_host, sizeof(g_boys_host))) ||
+      (s = up(o_ftab, B.h_ftab.data(), B.h_ftab.size() * sizeof(long long))))
     return s;
   // the previous call's counters are still in the array: clear them
   if ((s = cuda_status(cudaMemsetAsync(base + o_counts, 0, nblk * sizeof(int), st),
@@ -202,6 +204,7 @@ extern "C" int gbx_eri_full_noalloc(int n_shells, const int* angmom, const int* 
   e.blocks = reinterpret_cast<const BlockDev*>(base + o_blocks);
   e.compact = d_compact;
   e.out = out;
+  e.ftab = reinterpret_cast<const long long*>(base + o_ftab);
   const long long rows = B.nbf * B.nbf * B.nbf;
   const int grid = (int)std::max<long long>(1, std::min<long long>((rows + 7) / 8, (long long)nsm * 16));
   expand_full<<<grid, 256, 0, st>>>(e);

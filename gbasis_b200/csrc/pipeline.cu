@@ -105,34 +105,55 @@ __device__ __forceinline__ long long pair_row(const ExpandArgs& e, int s1, int c
   return (long long)info.z + ((pe & 1) ? (long long)c2 * info.w + c1 : (long long)c1 * info.w + c2);
 }
 
+// Function-pair key: class (bits 56..63), index of the shell pair within its class
+// (bits 32..55) and row of the ordered function pair in that class's block matrix
+// (bits 0..31).  One key per ordered pair of basis functions, built on the host.
+__device__ __forceinline__ int fk_cls(long long k) { return (int)(k >> 56); }
+__device__ __forceinline__ int fk_loc(long long k) { return (int)((k >> 32) & 0xffffff); }
+__device__ __forceinline__ long long fk_row(long long k) { return k & 0xffffffffLL; }
+
 __global__ void __launch_bounds__(256) expand_full(const ExpandArgs e) {
+  __shared__ long long s_base[kNumPairClasses * kNumPairClasses];
+  __shared__ long long s_ncols[kNumPairClasses * kNumPairClasses];
+  for (int i = threadIdx.x; i < kNumPairClasses * kNumPairClasses; i += blockDim.x) {
+    s_base[i] = e.blocks[i].base;
+    s_ncols[i] = e.blocks[i].ncols;
+  }
+  __syncthreads();
   const int lane = threadIdx.x & 31;
-  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  const long long n = e.n;
-  const long long rows = n * n * n;
-  for (long long r = warp; r < rows; r += nwarps) {
-    const long long i0 = r / (n * n), i1 = (r / n) % n, i2 = r % n;
-    // chemist: (a,b,c) = (i0,i1,i2); physicist out[i,j,k,l] = (ik|jl): (a,b,c) = (i0,i2,i1)
-    const int a = (int)i0;
-    const int b = (int)(e.notation == GBX_PHYSICIST ? i2 : i1);
-    const int c = (int)(e.notation == GBX_PHYSICIST ? i1 : i2);
-    int4 ip;
-    const long long rowp = pair_row(e, e.fsh[a], e.fcomp[a], e.fsh[b], e.fcomp[b], ip);
-    const int sc = e.fsh[c], cc = e.fcomp[c];
-    double* __restrict__ orow = e.out + r * n;
-    for (int d = lane; d < n; d += 32) {
-      int4 iq;
-      const long long rowq = pair_row(e, sc, cc, e.fsh[d], e.fcomp[d], iq);
-      long long off;
-      if (ip.x > iq.x || (ip.x == iq.x && ip.y >= iq.y)) {
-        const BlockDev bk = e.blocks[ip.x * kNumPairClasses + iq.x];
-        off = bk.base + rowp * bk.ncols + rowq;
-      } else {
-        const BlockDev bk = e.blocks[iq.x * kNumPairClasses + ip.x];
-        off = bk.base + rowq * bk.ncols + rowp;
+  const int warp = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nwarps = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+  const int n = (int)e.n;
+  const bool phys = e.notation == GBX_PHYSICIST;
+  // a warp takes whole planes out[i0, i1, :, :]; chemist rows are (a,b,c) = (i0,i1,i2),
+  // physicist out[i,j,k,l] = (ik|jl) rows are (a,b,c) = (i0,i2,i1)
+  for (int pl = warp; pl < n * n; pl += nwarps) {
+    const int i0 = pl / n, i1 = pl - i0 * n;
+    double* __restrict__ oplane = e.out + (long long)pl * n * n;
+    long long kp = phys ? 0 : e.ftab[(long long)i0 * n + i1];
+    const long long* __restrict__ qrow = e.ftab + (long long)(phys ? i1 : 0) * n;
+    for (int i2 = 0; i2 < n; ++i2) {
+      if (phys) kp = e.ftab[(long long)i0 * n + i2];
+      else qrow = e.ftab + (long long)i2 * n;
+      const unsigned hp = (unsigned)(kp >> 32);
+      const int cp = (int)(hp >> 24), lp = (int)(hp & 0xffffffu);
+      const unsigned rowp = (unsigned)kp;
+      double* __restrict__ orow = oplane + (long long)i2 * n;
+      for (int d = lane; d < n; d += 32) {
+        const long long kq = __ldg(qrow + d);
+        const unsigned hq = (unsigned)(kq >> 32);
+        const int cq = (int)(hq >> 24), lq = (int)(hq & 0xffffffu);
+        const unsigned rowq = (unsigned)kq;
+        long long off;
+        if (cp > cq || (cp == cq && lp >= lq)) {
+          const int t = cp * kNumPairClasses + cq;
+          off = s_base[t] + (long long)rowp * s_ncols[t] + rowq;
+        } else {
+          const int t = cq * kNumPairClasses + cp;
+          off = s_base[t] + (long long)rowq * s_ncols[t] + rowp;
+        }
+        orow[d] = __ldg(e.compact + off);
       }
-      orow[d] = __ldg(e.compact + off);
     }
   }
 }
@@ -224,6 +245,10 @@ int upload_basis(Basis& B) {
   if ((s = B.alloc((void**)&B.d_pinfo, np * sizeof(int4), "cudaMalloc(pinfo)"))) return s;
   GBX_CUDA(cudaMemcpy(B.d_pinfo, pinfo.data(), np * sizeof(int4), cudaMemcpyHostToDevice),
            "upload pinfo");
+  if ((s = B.alloc((void**)&B.d_ftab, B.h_ftab.size() * sizeof(long long), "cudaMalloc(ftab)")))
+    return s;
+  GBX_CUDA(cudaMemcpy(B.d_ftab, B.h_ftab.data(), B.h_ftab.size() * sizeof(long long),
+                      cudaMemcpyHostToDevice), "upload ftab");
   if ((s = B.alloc((void**)&B.d_q, np * sizeof(double), "cudaMalloc(q)"))) return s;
   if ((s = B.alloc((void**)&B.d_qscreen, np * sizeof(double), "cudaMalloc(qscreen)"))) return s;
   if ((s = boys_table(B.device, &B.d_boys))) return s;
@@ -326,7 +351,27 @@ int run_compact(Basis& B, double tau, cudaStream_t st) {
   GBX_CUDA(cudaGetLastError(), "build_work launch");
   if (B.profiling) cudaEventRecord(B.ev[1], st);
   const int nsm = num_sms(B.device);
-  for (int k = 0; k < nblk; ++k) {
+  // Class blocks are independent: spread them over the basis's auxiliary streams (largest
+  // first) so that small and latency-bound classes overlap; per-block timing runs them in
+  // order on the caller's stream instead.
+  const bool per_block = B.profiling && B.profile_level >= 2;
+  const int nstreams = per_block ? 0 : kAuxStreams;
+  if (nstreams) {
+    if (B.aux.empty()) {
+      B.aux.resize(nstreams);
+      B.join.resize(nstreams);
+      for (int j = 0; j < nstreams; ++j) {
+        GBX_CUDA(cudaStreamCreateWithFlags(&B.aux[j], cudaStreamNonBlocking), "create stream");
+        GBX_CUDA(cudaEventCreateWithFlags(&B.join[j], cudaEventDisableTiming), "create event");
+      }
+      GBX_CUDA(cudaEventCreateWithFlags(&B.fork, cudaEventDisableTiming), "create event");
+    }
+    GBX_CUDA(cudaEventRecord(B.fork, st), "fork");
+    for (int j = 0; j < nstreams; ++j) GBX_CUDA(cudaStreamWaitEvent(B.aux[j], B.fork, 0), "fork wait");
+  }
+  for (int i = 0; i < nblk; ++i) {
+    const int k = B.launch_order.empty() ? i : B.launch_order[i];
+    const cudaStream_t bs = nstreams ? B.aux[i % nstreams] : st;
     const HostBlock& h = B.blocks[k];
     int la, lb, lc, ld;
     class_dims(h.cb, la, lb);
@@ -339,8 +384,18 @@ int run_compact(Basis& B, double tau, cudaStream_t st) {
     a.base = h.dev.base;
     a.ncols = h.dev.ncols;
     a.mode = 0;
-    const int grid = (int)std::min<long long>((h.ncand + 127) / 128, (long long)nsm * 8);
-    if ((s = launch_class(la, lb, lc, ld, a, grid, st))) return s;
+    a.team = h.team;
+    const int grid =
+        (int)std::max<long long>(1, std::min<long long>((h.ncand * h.team + 127) / 128, (long long)nsm * 8));
+    if (per_block) cudaEventRecord(B.blk_ev[i], st);
+    if ((s = launch_class(la, lb, lc, ld, a, grid, bs))) return s;
+  }
+  if (per_block) cudaEventRecord(B.blk_ev[nblk], st);
+  if (nstreams) {
+    for (int j = 0; j < nstreams; ++j) {
+      GBX_CUDA(cudaEventRecord(B.join[j], B.aux[j]), "join");
+      GBX_CUDA(cudaStreamWaitEvent(st, B.join[j], 0), "join wait");
+    }
   }
   return GBX_OK;
 }
@@ -359,6 +414,7 @@ int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st) {
   e.blocks = B.d_blocks;
   e.compact = B.d_compact;
   e.out = out;
+  e.ftab = B.d_ftab;
   const long long rows = (long long)B.nbf * B.nbf * B.nbf;
   const int grid = (int)std::max<long long>(1, std::min<long long>((rows + 7) / 8,
                                                                     (long long)num_sms(B.device) * 16));

@@ -22,6 +22,7 @@ struct ExpandArgs {
   const BlockDev* blocks;
   const double* compact;
   double* out;
+  const long long* ftab;  // n*n function-pair keys (class, pair index in class, block row)
 };
 
 __global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,

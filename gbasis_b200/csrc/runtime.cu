@@ -107,6 +107,13 @@ Basis::~Basis() {
   for (void* p : dev_allocs) free_dev(p);
   for (cudaEvent_t& e : ev)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t& e : blk_ev)
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t& x : aux)
+    if (x) cudaStreamDestroy(x);
+  for (cudaEvent_t& e : join)
+    if (e) cudaEventDestroy(e);
+  if (fork) cudaEventDestroy(fork);
 }
 
 int Basis::alloc(void** p, size_t bytes, const char* what) {
@@ -254,6 +261,55 @@ int build_basis(Basis& B, int n, const int* angmom, const int* nprim, const doub
     }
   B.compact_elems = base;
   B.n_quartets = work;
+  // function-pair keys of the expansion: (class << 56) | (index in class << 32) | block row
+  {
+    std::vector<int> fsh(B.nbf), fcomp(B.nbf);
+    for (int sh = 0; sh < n; ++sh)
+      for (int c = 0; c < B.shells[sh].nout; ++c) {
+        fsh[B.shells[sh].func_off + c] = sh;
+        fcomp[B.shells[sh].func_off + c] = c;
+      }
+    B.h_ftab.resize((size_t)B.nbf * B.nbf);
+    for (long long x = 0; x < B.nbf; ++x)
+      for (long long y = 0; y < B.nbf; ++y) {
+        const int pe = B.pair_of[(size_t)fsh[x] * n + fsh[y]];
+        const PairDev& p = B.pairs[pe >> 1];
+        const long long row = p.fo + ((pe & 1) ? (long long)fcomp[y] * p.nB + fcomp[x]
+                                               : (long long)fcomp[x] * p.nB + fcomp[y]);
+        B.h_ftab[(size_t)x * B.nbf + y] =
+            ((long long)p.cls << 56) | ((long long)p.local << 32) | row;
+      }
+  }
+  // default lanes-per-quartet: about four primitive quartets per lane, fewer lanes when the
+  // accumulator set (reduced across the team by shuffles) is large
+  std::vector<double> cprims(kNumPairClasses, 0.0);
+  for (const PairDev& p : B.pairs) cprims[p.cls] += p.nprim;
+  for (int c = 0; c < kNumPairClasses; ++c)
+    if (B.class_count[c]) cprims[c] /= (double)B.class_count[c];
+  for (HostBlock& h : B.blocks) {
+    h.avg_prims = cprims[h.cb] * cprims[h.ck];
+    const int la = kPairClassL[h.cb][0], lb = kPairClassL[h.cb][1];
+    const int lc = kPairClassL[h.ck][0], ld = kPairClassL[h.ck][1];
+    int ne = 0, nf = 0;
+    for (int e = la; e <= la + lb; ++e) ne += ncart(e);
+    for (int f = lc; f <= lc + ld; ++f) nf += ncart(f);
+    const int cap = ne * nf > 100 ? 2 : (ne * nf > 40 ? 8 : 32);
+    int t = 1;
+    while (t < cap && h.avg_prims / (2 * t) >= 4.0) t *= 2;
+    h.team = t;
+  }
+  // launch order: estimated work, largest first
+  std::vector<double> cost(B.blocks.size());
+  for (size_t k = 0; k < B.blocks.size(); ++k) {
+    const HostBlock& h = B.blocks[k];
+    const int la = kPairClassL[h.cb][0], lb = kPairClassL[h.cb][1];
+    const int lc = kPairClassL[h.ck][0], ld = kPairClassL[h.ck][1];
+    cost[k] = (double)h.ncand * (h.avg_prims + 4.0) * ncart(la) * ncart(lb) * ncart(lc) * ncart(ld);
+  }
+  B.launch_order.resize(B.blocks.size());
+  for (size_t k = 0; k < B.blocks.size(); ++k) B.launch_order[k] = (int)k;
+  std::stable_sort(B.launch_order.begin(), B.launch_order.end(),
+                   [&](int x, int y) { return cost[x] > cost[y]; });
   return GBX_OK;
 }
 
@@ -370,7 +426,12 @@ int gbx_set_profiling(gbx_basis* b, int on) {
   DeviceGuard g(B.device);
   if (on && !B.ev[0])
     for (cudaEvent_t& e : B.ev) GBX_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+  if (on && B.blk_ev.empty()) {
+    B.blk_ev.resize(B.blocks.size() + 1);
+    for (cudaEvent_t& e : B.blk_ev) GBX_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+  }
   B.profiling = on != 0;
+  B.profile_level = on;
   return GBX_OK;
 }
 
@@ -384,6 +445,57 @@ int gbx_phase_times(gbx_basis* b, double* ms) {
     float t = 0.f;
     GBX_CUDA(cudaEventElapsedTime(&t, B.ev[i], B.ev[i + 1]), "phase elapsed time");
     ms[i] = t;
+  }
+  return GBX_OK;
+}
+
+int gbx_num_blocks(const gbx_basis* b, int* n) {
+  if (!b || !n) return set_error(GBX_ERR_INVALID, "gbx_num_blocks: null argument");
+  *n = (int)b->impl->blocks.size();
+  return GBX_OK;
+}
+
+int gbx_block_info(const gbx_basis* b, int k, int* cls4, int* team, double* avg_prims,
+                   int64_t* n_quartets) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_block_info: null basis");
+  const Basis& B = *b->impl;
+  if (k < 0 || k >= (int)B.blocks.size()) return set_error(GBX_ERR_INVALID, "block %d out of range", k);
+  const HostBlock& h = B.blocks[k];
+  if (cls4) {
+    cls4[0] = kPairClassL[h.cb][0];
+    cls4[1] = kPairClassL[h.cb][1];
+    cls4[2] = kPairClassL[h.ck][0];
+    cls4[3] = kPairClassL[h.ck][1];
+  }
+  if (team) *team = h.team;
+  if (avg_prims) *avg_prims = h.avg_prims;
+  if (n_quartets) *n_quartets = h.ncand;
+  return GBX_OK;
+}
+
+int gbx_set_team(gbx_basis* b, int k, int team) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_set_team: null basis");
+  Basis& B = *b->impl;
+  if (k < 0 || k >= (int)B.blocks.size()) return set_error(GBX_ERR_INVALID, "block %d out of range", k);
+  if (team < 1 || team > 32 || (team & (team - 1)))
+    return set_error(GBX_ERR_INVALID, "team must be a power of two in [1, 32]");
+  B.blocks[k].team = team;
+  return GBX_OK;
+}
+
+int gbx_block_times(gbx_basis* b, double* ms, int n) {
+  if (!b || !ms) return set_error(GBX_ERR_INVALID, "gbx_block_times: null argument");
+  Basis& B = *b->impl;
+  if (!B.profiling || B.blk_ev.empty())
+    return set_error(GBX_ERR_INVALID, "profiling is off for this basis");
+  if (n < (int)B.blocks.size()) return set_error(GBX_ERR_INVALID, "array too short");
+  DeviceGuard g(B.device);
+  GBX_CUDA(cudaEventSynchronize(B.blk_ev.back()), "block events");
+  if (B.profile_level < 2) return set_error(GBX_ERR_INVALID, "per-block timing needs level 2");
+  for (size_t i = 0; i < B.blocks.size(); ++i) {
+    float t = 0.f;
+    GBX_CUDA(cudaEventElapsedTime(&t, B.blk_ev[i], B.blk_ev[i + 1]), "block elapsed time");
+    ms[B.launch_order.empty() ? i : B.launch_order[i]] = t;
   }
   return GBX_OK;
 }

@@ -10,6 +10,8 @@
 
 namespace gbx {
 
+constexpr int kAuxStreams = 6;
+
 int boys_table(int device, const double** out);
 int compiled_lmax();
 
@@ -18,6 +20,8 @@ struct HostBlock {
   long long nb, nk, ncand;
   bool tri;
   BlockDev dev;
+  double avg_prims = 1.0;  // mean primitive quartets per shell quartet
+  int team = 1;            // lanes per quartet (register kernel), set by heuristic or autotuner
 };
 
 struct Basis {
@@ -29,6 +33,8 @@ struct Basis {
   std::vector<PairDev> pairs;
   std::vector<int> pair_of;  // n*n: (pair << 1) | (first index on B shell)
   std::vector<int> group;    // original (generalized) shell of each segmented shell
+  std::vector<long long> h_ftab;  // nbf*nbf function-pair keys of the expansion
+  long long* d_ftab = nullptr;
   std::vector<long long> class_first, class_count, class_funcs;
   std::vector<HostBlock> blocks;
   std::vector<BlockDev> block_table;  // kNumPairClasses^2, base = -1 when empty
@@ -64,6 +70,12 @@ struct Basis {
   // [0] work-list build, [1] class kernels, [2] expansion
   bool profiling = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> blk_ev;  // per class-block launch (profiling level 2), launch order
+  int profile_level = 0;
+  std::vector<int> launch_order;    // class blocks, largest estimated cost first
+  std::vector<cudaStream_t> aux;    // concurrent class-block streams
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
   std::vector<void*> dev_allocs;
 
   ~Basis();

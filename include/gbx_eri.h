@@ -125,11 +125,22 @@ int gbx_eri_coulomb_j(gbx_basis* b, const double* D, double schwarz_threshold, d
 /* Device-side counters of the last call on this basis: quartets computed and screened. */
 int gbx_last_counts(const gbx_basis* b, int64_t* computed, int64_t* screened);
 
-/* Phase timing: when on, full-tensor calls record CUDA events on their stream around the
- * work-list build, the class kernels and the expansion; gbx_phase_times waits for the last
- * call and returns the three durations in milliseconds. */
+/* Phase timing: level 1 records CUDA events on the call's stream around the work-list
+ * build, the class kernels and the expansion (gbx_phase_times waits for the last call and
+ * returns the three durations in ms); level 2 also times every class block, running them
+ * one after another on the call's stream instead of concurrently; 0 turns it off. */
 int gbx_set_profiling(gbx_basis* b, int on);
 int gbx_phase_times(gbx_basis* b, double* ms3);
+
+/* Work decomposition per class block (the autotuner's knobs): a class block is the set of
+ * quartets of one (bra pair class, ket pair class); `team` is how many lanes share one
+ * quartet's primitive loop in the register kernel (power of two, 1..32).  With profiling on,
+ * gbx_block_times returns each block's kernel time of the last call (ms). */
+int gbx_num_blocks(const gbx_basis* b, int* n);
+int gbx_block_info(const gbx_basis* b, int k, int* cls4, int* team, double* avg_prims,
+                   int64_t* n_quartets);
+int gbx_set_team(gbx_basis* b, int k, int team);
+int gbx_block_times(gbx_basis* b, double* ms, int n);
 
 /* Copy of the last error message on this thread (NUL-terminated, truncated to len). */
 int gbx_last_error(char* buf, size_t len);
