@@ -1,0 +1,43 @@
+"""Direct Coulomb matrix J_ab = sum_cd (ab|cd) D_cd on the GPU.
+
+The ERI tensor is never stored: screened unique shell quartets (Schwarz bound
+Q_ab Q_cd >= ``schwarz_threshold``, bounds on blocks without ``norm_cont`` as gbasis's
+``SchwarzScreener`` uses, ``gbasis/integrals/_schwarz_screening.py:14-191``) are evaluated
+in chunks and contracted with D as they are produced (``gbx_eri_coulomb_j``).  gbasis has no
+direct counterpart; it is the contraction users apply to ``electron_repulsion_integral``'s
+chemist tensor, ``einsum("abcd,cd->ab", eri, D)``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _engine
+
+__all__ = ["coulomb_matrix"]
+
+
+def coulomb_matrix(basis, density, schwarz_threshold=1e-12, coord_type=None, device=None):
+    """J (K, K) float64 for the symmetric density ``density`` (K, K) in the basis's
+    functions (coordinate types from the shells unless ``coord_type`` overrides them)."""
+    import torch
+    types = None
+    if coord_type is not None:
+        types = [coord_type] * len(basis) if isinstance(coord_type, str) else list(coord_type)
+    db = _engine.DeviceBasis(list(basis), types, device=device)
+    try:
+        n = db.nbf
+        D = np.ascontiguousarray(density, dtype=np.float64)
+        if D.shape != (n, n):
+            raise ValueError(f"`density` must have shape ({n}, {n})")
+        dev = torch.device("cuda", db.device)
+        d_D = torch.from_numpy(D).to(dev)
+        d_J = torch.empty((n, n), dtype=torch.float64, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _engine.check(_engine.lib().gbx_eri_coulomb_j(
+            db.handle, ctypes.c_void_p(d_D.data_ptr()), float(schwarz_threshold),
+            ctypes.c_void_p(d_J.data_ptr()), ctypes.c_void_p(stream)), "gbx_eri_coulomb_j")
+        return d_J.cpu().numpy()
+    finally:
+        db.close()

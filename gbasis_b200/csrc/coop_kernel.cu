@@ -140,6 +140,8 @@ __global__ void eri_coop(const CoopArgs A) {
   double* BN = KN;
   double* OB = BN + A.Cc * M.nB;
   double* T2 = OB + A.Cc * NAB;
+  double* VAB = T2 + A.Cc * NAB;  // Coulomb mode: sum_cd (ab|cd) D[c][d] per (a, b)
+  double* DAB = VAB + NAB;        // Coulomb mode: D[a][b] of the bra block
 
   const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
@@ -223,9 +225,19 @@ __global__ void eri_coop(const CoopArgs A) {
     const ShellDev& sC = a.shells[Q.shA];
     const ShellDev& sD = a.shells[Q.shB];
     const bool schwarz = a.mode == 1;  // Cartesian block, max |(ab|ab)| with component norms
+    const bool coulomb = a.mode == 2;  // accumulate J instead of storing the block
     const int nAi = schwarz ? NCA : n_int(sA), nBi = schwarz ? NCB : n_int(sB);
     const int nCi = schwarz ? NCC : n_int(sC), nDi = schwarz ? NCDD : n_int(sD);
     double mx = 0.0;
+    if (coulomb) {
+      for (int i = lane; i < nAi * nBi; i += 32) {
+        const int ua = i / nBi, ub = i - ua * nBi;
+        VAB[i] = 0.0;
+        DAB[i] = a.D[(sA.func_off + sA.pos[ua]) * a.nbf + sB.func_off + sB.pos[ub]] *
+                 sA.scl[ua] * sB.scl[ub];
+      }
+      __syncwarp();
+    }
     // ---------------------------------------------------------------- C
     if (nCi != NCC || nDi != NCDD) {
       for (int e = 0; e < M.NE; ++e) {
@@ -311,6 +323,33 @@ __global__ void eri_coop(const CoopArgs A) {
         for (int i = lane; i < cc * NAB; i += 32) OB[i] = T2[i];
       }
       __syncwarp();
+      if (coulomb) {
+        // J[a][b] partial sums over this chunk's columns; J[c][d] of each column
+        const int nab = nAi * nBi;
+        for (int i = lane; i < nab; i += 32) {
+          double s = VAB[i];
+          for (int c = 0; c < cc; ++c) {
+            const int col = c0 + c, uc = col / nDi, ud = col - uc * nDi;
+            const double dcd = a.D[(sC.func_off + sC.pos[uc]) * a.nbf + sD.func_off + sD.pos[ud]] *
+                               sC.scl[uc] * sD.scl[ud];
+            s = fma(OB[c * NAB + i], dcd, s);
+          }
+          VAB[i] = s;
+        }
+        if (pq.x != pq.y) {
+          for (int c = lane; c < cc; c += 32) {
+            const int col = c0 + c, uc = col / nDi, ud = col - uc * nDi;
+            double s = 0.0;
+            for (int i = 0; i < nab; ++i) s = fma(OB[c * NAB + i], DAB[i], s);
+            s *= ((P.shA != P.shB) ? 2.0 : 1.0) * sC.scl[uc] * sD.scl[ud];
+            const long long fc = sC.func_off + sC.pos[uc], fd = sD.func_off + sD.pos[ud];
+            atomicAdd(a.J + fc * a.nbf + fd, s);
+            if (Q.shA != Q.shB) atomicAdd(a.J + fd * a.nbf + fc, s);
+          }
+        }
+        __syncwarp();
+        continue;
+      }
       for (int i = lane; i < cc * nAi * nBi; i += 32) {
         const int c = i / (nAi * nBi), rem = i - c * nAi * nBi, ua = rem / nBi, ub = rem - ua * nBi;
         const int col = c0 + c, uc = col / nDi, ud = col - uc * nDi;
@@ -330,6 +369,16 @@ __global__ void eri_coop(const CoopArgs A) {
     if (schwarz) {
       for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
       if (lane == 0) a.qout[pq.x] = sqrt(mx);
+    }
+    if (coulomb) {
+      const double fk = (Q.shA != Q.shB) ? 2.0 : 1.0;
+      for (int i = lane; i < nAi * nBi; i += 32) {
+        const int ua = i / nBi, ub = i - ua * nBi;
+        const long long fa = sA.func_off + sA.pos[ua], fbn = sB.func_off + sB.pos[ub];
+        const double s = VAB[i] * fk * sA.scl[ua] * sB.scl[ub];
+        atomicAdd(a.J + fa * a.nbf + fbn, s);
+        if (P.shA != P.shB) atomicAdd(a.J + fbn * a.nbf + fa, s);
+      }
     }
     __syncwarp();
   }
@@ -355,7 +404,8 @@ int launch_coop(int prog, const EriLaunch& a, cudaStream_t st) {
     long long s = NENF + M.nX;
     s = std::max<long long>(s, NENF + (long long)M.NE * NCD + (long long)R * M.nK);
     s = std::max<long long>(s, NENF + (long long)M.NE * NCD + NCD);
-    s = std::max<long long>(s, NENF + (long long)M.NE * NCD + (long long)Cc * (M.nB + 2 * NAB));
+    s = std::max<long long>(s, NENF + (long long)M.NE * NCD + (long long)Cc * (M.nB + 2 * NAB) +
+                                   2 * NAB);
     return s;
   };
   int R = 8, Cc = 8;

@@ -99,6 +99,70 @@ __device__ __forceinline__ void stage_boys(const double* __restrict__ tab, doubl
     s_exp[n] = tab[n * (kBoysOrders + 1) + kBoysOrders];
 }
 
+// Coulomb-matrix epilogue of one unique quartet (bra pair shells A, B; ket C, D), block `v`
+// in internal order [NA][NB][NC][ND] after the spherical transforms.  Every ordered shell
+// quartet mapping to this unique one contributes:
+//   J[a][b] += (1 + [C != D]) sum_cd (ab|cd) D[c][d]      (and J[b][a] when A != B)
+//   J[c][d] += (1 + [A != B]) sum_ab (ab|cd) D[a][b]      (when bra pair != ket pair;
+//                                                           and J[d][c] when C != D)
+template <int NA, int NB, int NC, int ND>
+__device__ __forceinline__ void coulomb_epilogue(const EriLaunch& a, int2 pq, const PairDev& P,
+                                                 const PairDev& Q, const ShellDev& sA,
+                                                 const ShellDev& sB, const ShellDev& sC,
+                                                 const ShellDev& sD, int nAi, int nBi, int nCi,
+                                                 int nDi, const double* v) {
+  const long long n = a.nbf;
+  const double fk = (Q.shA != Q.shB) ? 2.0 : 1.0;
+  const double fb = (P.shA != P.shB) ? 2.0 : 1.0;
+  const bool swap = pq.x != pq.y;
+  double dcd[NC * ND];
+  double w[NC * ND];
+#pragma unroll
+  for (int ic = 0; ic < NC; ++ic)
+#pragma unroll
+    for (int id = 0; id < ND; ++id) {
+      w[ic * ND + id] = 0.0;
+      dcd[ic * ND + id] = (ic < nCi && id < nDi)
+                              ? a.D[(sC.func_off + sC.pos[ic]) * n + sD.func_off + sD.pos[id]] *
+                                    sC.scl[ic] * sD.scl[id]
+                              : 0.0;
+    }
+#pragma unroll
+  for (int ia = 0; ia < NA; ++ia) {
+    if (ia >= nAi) break;
+#pragma unroll
+    for (int ib = 0; ib < NB; ++ib) {
+      if (ib >= nBi) break;
+      const long long fa = sA.func_off + sA.pos[ia], fbn = sB.func_off + sB.pos[ib];
+      const double sab = sA.scl[ia] * sB.scl[ib];
+      const double dab = a.D[fa * n + fbn] * sab;
+      double s = 0.0;
+#pragma unroll
+      for (int c = 0; c < NC * ND; ++c) {
+        const double x = v[(ia * NB + ib) * NC * ND + c];
+        s = fma(x, dcd[c], s);
+        w[c] = fma(x, dab, w[c]);
+      }
+      s *= fk * sab;
+      atomicAdd(a.J + fa * n + fbn, s);
+      if (P.shA != P.shB) atomicAdd(a.J + fbn * n + fa, s);
+    }
+  }
+  if (!swap) return;
+#pragma unroll
+  for (int ic = 0; ic < NC; ++ic) {
+    if (ic >= nCi) break;
+#pragma unroll
+    for (int id = 0; id < ND; ++id) {
+      if (id >= nDi) break;
+      const long long fc = sC.func_off + sC.pos[ic], fd = sD.func_off + sD.pos[id];
+      const double s = w[ic * ND + id] * fb * sC.scl[ic] * sD.scl[id];
+      atomicAdd(a.J + fc * n + fd, s);
+      if (Q.shA != Q.shB) atomicAdd(a.J + fd * n + fc, s);
+    }
+  }
+}
+
 template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(kEriThreads) eri_block_fp64(const EriLaunch a) {
   using C = gen::Cls<LA, LB, LC, LD>;
@@ -196,6 +260,10 @@ __global__ void __launch_bounds__(kEriThreads) eri_block_fp64(const EriLaunch a)
     if (LA >= 2 && sA.sph) sph_axis<LA, 1, NCB * NCC * NCD>(out);
     const int nAi = internal_count(sA), nBi = internal_count(sB);
     const int nCi = internal_count(sC), nDi = internal_count(sD);
+    if (a.mode == 2) {
+      coulomb_epilogue<NCA, NCB, NCC, NCD>(a, pq, P, Q, sA, sB, sC, sD, nAi, nBi, nCi, nDi, out);
+      continue;
+    }
     const long long nBo = sB.nout, nDo = sD.nout;
     double* __restrict__ dst = a.out + a.base + Q.fo;
 #pragma unroll

@@ -9,6 +9,10 @@
 
 using namespace gbx;
 
+namespace gbx {
+int coulomb_entry(gbx_basis* b, const double* D, double tau, double* J, cudaStream_t st);
+}
+
 namespace {
 
 struct CublasHandle {
@@ -101,8 +105,9 @@ int gbx_fp64_peak(int device, double* tflops) {
 }
 
 int gbx_eri_coulomb_j(gbx_basis* b, const double* D, double tau, double* J, void* stream) {
-  (void)b; (void)D; (void)tau; (void)J; (void)stream;
-  return set_error(GBX_ERR_UNSUPPORTED, "gbx_eri_coulomb_j: not built yet");
+  if (!b || !D || !J) return set_error(GBX_ERR_INVALID, "gbx_eri_coulomb_j: null argument");
+  if (!(tau >= 0.0)) return set_error(GBX_ERR_INVALID, "schwarz threshold must be >= 0");
+  return gbx::coulomb_entry(b, D, tau, J, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -81,6 +81,10 @@ struct EriLaunch {
   long long base, ncols;
   int mode;                 // 0 = write block, 1 = Schwarz diagonal (max |.| -> qout)
   int team;                 // lanes per quartet in the register kernel (1..32, power of two)
+  // mode 2 (Coulomb matrix): J[a][b] += sum_cd (ab|cd) D[c][d] over the unique quartets
+  const double* D;          // nbf x nbf, symmetric
+  double* J;                // nbf x nbf, accumulated with atomics
+  long long nbf;
   double* qout;             // per-pair Schwarz value (mode 1)
   int* status;              // device error flag
 };

@@ -63,6 +63,37 @@ __global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,
 }
 
 // ------------------------------------------------------------------- K2
+// Candidates [start, start + len) of one class block: Schwarz test, warp-ballot compaction
+// into work[0..count) (the direct Coulomb path processes the quartet space in chunks).
+__global__ void build_work_range(const BuildBlock B, long long start, long long len,
+                                 const double* __restrict__ qs, double tau,
+                                 int2* __restrict__ work, int* __restrict__ count) {
+  const long long t = start + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool pass = false;
+  int p = 0, q = 0;
+  if (t < start + len && t < B.ncand) {
+    long long pl, ql;
+    if (B.tri) {
+      pl = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+      while (pl * (pl + 1) / 2 > t) --pl;
+      while ((pl + 1) * (pl + 2) / 2 <= t) ++pl;
+      ql = t - pl * (pl + 1) / 2;
+    } else {
+      pl = t / B.nk;
+      ql = t - pl * B.nk;
+    }
+    p = B.pb0 + (int)pl;
+    q = B.pk0 + (int)ql;
+    pass = (tau <= 0.0) || (qs[p] * qs[q] >= tau);
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, pass);
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0 && mask) base = atomicAdd(count, __popc(mask));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (pass) work[base + __popc(mask & ((1u << lane) - 1u))] = make_int2(p, q);
+}
+
 __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* __restrict__ bb,
                            const double* __restrict__ qs, double tau, int2* __restrict__ work,
                            int* __restrict__ counts) {
@@ -212,11 +243,32 @@ int upload_basis(Basis& B) {
   GBX_CUDA(cudaMemcpy(B.d_blocks, B.block_table.data(), B.block_table.size() * sizeof(BlockDev),
                       cudaMemcpyHostToDevice), "upload blocks");
 
-  // work list + build map
-  if ((s = B.alloc((void**)&B.d_work, (size_t)B.n_quartets * sizeof(int2), "cudaMalloc(work)")))
-    return s;
   const int nblk = (int)B.blocks.size();
   if ((s = B.alloc((void**)&B.d_counts, (nblk + 4) * sizeof(int), "cudaMalloc(counts)"))) return s;
+  if ((s = B.alloc((void**)&B.d_pinfo, np * sizeof(int4), "cudaMalloc(pinfo)"))) return s;
+  std::vector<int4> pinfo(np);
+  for (int p = 0; p < np; ++p)
+    pinfo[p] = make_int4(B.pairs[p].cls, B.pairs[p].local, B.pairs[p].fo, B.pairs[p].nB);
+  GBX_CUDA(cudaMemcpy(B.d_pinfo, pinfo.data(), np * sizeof(int4), cudaMemcpyHostToDevice),
+           "upload pinfo");
+  if ((s = B.alloc((void**)&B.d_ftab, B.h_ftab.size() * sizeof(long long), "cudaMalloc(ftab)")))
+    return s;
+  GBX_CUDA(cudaMemcpy(B.d_ftab, B.h_ftab.data(), B.h_ftab.size() * sizeof(long long),
+                      cudaMemcpyHostToDevice), "upload ftab");
+  if ((s = B.alloc((void**)&B.d_q, np * sizeof(double), "cudaMalloc(q)"))) return s;
+  if ((s = B.alloc((void**)&B.d_qscreen, np * sizeof(double), "cudaMalloc(qscreen)"))) return s;
+  if ((s = boys_table(B.device, &B.d_boys))) return s;
+  GBX_CUDA(cudaDeviceSynchronize(), "basis upload");
+  return GBX_OK;
+}
+
+// Work list and build map of a full-tensor call (every unique quartet), made on first use.
+static int ensure_full_work(Basis& B) {
+  if (B.d_work) return GBX_OK;
+  int s;
+  const int nblk = (int)B.blocks.size();
+  if ((s = B.alloc((void**)&B.d_work, (size_t)B.n_quartets * sizeof(int2), "cudaMalloc(work)")))
+    return s;
   std::vector<BuildBlock> bb(nblk);
   std::vector<int2> cmap;
   for (int k = 0; k < nblk; ++k) {
@@ -238,21 +290,6 @@ int upload_basis(Basis& B) {
   GBX_CUDA(cudaMemcpy(B.d_cta_map, cmap.data(), cmap.size() * sizeof(int2), cudaMemcpyHostToDevice),
            "upload cta map");
   B.d_build_blocks = dbb;
-
-  std::vector<int4> pinfo(np);
-  for (int p = 0; p < np; ++p)
-    pinfo[p] = make_int4(B.pairs[p].cls, B.pairs[p].local, B.pairs[p].fo, B.pairs[p].nB);
-  if ((s = B.alloc((void**)&B.d_pinfo, np * sizeof(int4), "cudaMalloc(pinfo)"))) return s;
-  GBX_CUDA(cudaMemcpy(B.d_pinfo, pinfo.data(), np * sizeof(int4), cudaMemcpyHostToDevice),
-           "upload pinfo");
-  if ((s = B.alloc((void**)&B.d_ftab, B.h_ftab.size() * sizeof(long long), "cudaMalloc(ftab)")))
-    return s;
-  GBX_CUDA(cudaMemcpy(B.d_ftab, B.h_ftab.data(), B.h_ftab.size() * sizeof(long long),
-                      cudaMemcpyHostToDevice), "upload ftab");
-  if ((s = B.alloc((void**)&B.d_q, np * sizeof(double), "cudaMalloc(q)"))) return s;
-  if ((s = B.alloc((void**)&B.d_qscreen, np * sizeof(double), "cudaMalloc(qscreen)"))) return s;
-  if ((s = boys_table(B.device, &B.d_boys))) return s;
-  GBX_CUDA(cudaDeviceSynchronize(), "basis upload");
   return GBX_OK;
 }
 
@@ -337,6 +374,7 @@ int ensure_schwarz(Basis& B, cudaStream_t st) {
 int run_compact(Basis& B, double tau, cudaStream_t st) {
   int s;
   if (tau > 0.0 && (s = ensure_schwarz(B, st))) return s;
+  if ((s = ensure_full_work(B))) return s;
   if ((s = B.ensure_scratch(B.compact_elems, 0))) return s;
   const int nblk = (int)B.blocks.size();
   GBX_CUDA(cudaMemsetAsync(B.d_counts, 0, nblk * sizeof(int), st), "clear counts");
@@ -397,6 +435,55 @@ int run_compact(Basis& B, double tau, cudaStream_t st) {
       GBX_CUDA(cudaStreamWaitEvent(st, B.join[j], 0), "join wait");
     }
   }
+  return GBX_OK;
+}
+
+// Direct Coulomb matrix: the unique quartets of every class block, in chunks of
+// kCoulombChunk candidates (Schwarz-screened and compacted by build_work_range), feed the
+// class kernels in mode 2, which accumulate J with atomics.  No integral is stored.
+int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st) {
+  int s;
+  if (tau > 0.0 && (s = ensure_schwarz(B, st))) return s;
+  const long long chunk = kCoulombChunk;
+  if (!B.d_jwork) {
+    if ((s = B.alloc((void**)&B.d_jwork, (size_t)chunk * sizeof(int2), "cudaMalloc(J work)")))
+      return s;
+  }
+  GBX_CUDA(cudaMemsetAsync(J, 0, (size_t)B.nbf * B.nbf * sizeof(double), st), "clear J");
+  const int nsm = num_sms(B.device);
+  const int nblk = (int)B.blocks.size();
+  long long computed = 0;
+  for (int i = 0; i < nblk; ++i) {
+    const int k = B.launch_order.empty() ? i : B.launch_order[i];
+    const HostBlock& h = B.blocks[k];
+    const BuildBlock bb{(int)B.class_first[h.cb], (int)h.nb, (int)B.class_first[h.ck], (int)h.nk,
+                        h.tri ? 1 : 0, k, 0, h.ncand};
+    for (long long start = 0; start < h.ncand; start += chunk) {
+      const long long len = std::min(chunk, h.ncand - start);
+      int* cnt = B.d_counts + k;
+      GBX_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), st), "clear chunk count");
+      build_work_range<<<(int)((len + 255) / 256), 256, 0, st>>>(bb, start, len, B.d_qscreen, tau,
+                                                                 B.d_jwork, cnt);
+      GBX_CUDA(cudaGetLastError(), "build_work_range launch");
+      EriLaunch a = base_launch(B);
+      a.work = B.d_jwork;
+      a.work_count = cnt;
+      a.work_off = 0;
+      a.nwork = len;
+      a.mode = 2;
+      a.team = h.team;
+      a.D = D;
+      a.J = J;
+      a.nbf = B.nbf;
+      const int grid =
+          (int)std::max<long long>(1, std::min<long long>((len * h.team + 127) / 128, (long long)nsm * 8));
+      if ((s = launch_class(kPairClassL[h.cb][0], kPairClassL[h.cb][1], kPairClassL[h.ck][0],
+                            kPairClassL[h.ck][1], a, grid, st)))
+        return s;
+      computed += len;
+    }
+  }
+  (void)computed;
   return GBX_OK;
 }
 

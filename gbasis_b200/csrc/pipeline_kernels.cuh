@@ -33,5 +33,8 @@ __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* _
                            const double* __restrict__ qs, double tau, int2* __restrict__ work,
                            int* __restrict__ counts);
 __global__ void expand_full(const ExpandArgs e);
+__global__ void build_work_range(const BuildBlock B, long long start, long long len,
+                                 const double* __restrict__ qs, double tau,
+                                 int2* __restrict__ work, int* __restrict__ count);
 
 }  // namespace gbx

@@ -321,6 +321,14 @@ struct gbx_basis {
   std::unique_ptr<Basis> impl;
 };
 
+namespace gbx {
+int coulomb_entry(gbx_basis* b, const double* D, double tau, double* J, cudaStream_t st) {
+  Basis& B = *b->impl;
+  DeviceGuard g(B.device);
+  return run_coulomb(B, D, tau, J, st);
+}
+}  // namespace gbx
+
 extern "C" {
 
 int gbx_last_error(char* buf, size_t len) {

@@ -11,6 +11,7 @@
 namespace gbx {
 
 constexpr int kAuxStreams = 6;
+constexpr long long kCoulombChunk = 1LL << 24;  // quartet candidates per Coulomb chunk
 
 int boys_table(int device, const double** out);
 int compiled_lmax();
@@ -35,6 +36,7 @@ struct Basis {
   std::vector<int> group;    // original (generalized) shell of each segmented shell
   std::vector<long long> h_ftab;  // nbf*nbf function-pair keys of the expansion
   long long* d_ftab = nullptr;
+  int2* d_jwork = nullptr;  // Coulomb chunk work list
   std::vector<long long> class_first, class_count, class_funcs;
   std::vector<HostBlock> blocks;
   std::vector<BlockDev> block_table;  // kNumPairClasses^2, base = -1 when empty
@@ -90,6 +92,7 @@ void boys_host_table(double* h);
 int upload_basis(Basis& B);
 int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st);
 int run_compact(Basis& B, double tau, cudaStream_t st);
+int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st);
 int ensure_schwarz(Basis& B, cudaStream_t st);
 int launch_class(int la, int lb, int lc, int ld, const EriLaunch& a, int grid, cudaStream_t st);
 
