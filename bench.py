@@ -237,6 +237,30 @@ def main():
         ms = float(t.item())
     value = world * n_unique / (ms * 1e-3)
 
+    # mixed-precision form on the same workload, and its error against the FP64 tensor
+    from gbasis_b200.electron_repulsion import MIXED_FP32, MIXED_SKIP
+    ref = out.clone()
+    mixed_args = (MIXED_SKIP, MIXED_FP32)
+
+    def step_mixed():
+        db.full_device(out.data_ptr(), "chemist", 0.0, stream=sp, mixed=mixed_args)
+
+    for _ in range(max(3, a.warmup)):
+        step_mixed()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(a.steps):
+        step_mixed()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_mixed = e0.elapsed_time(e1) / a.steps
+    err = (out - ref).abs()
+    mixed = {"value": world * n_unique / (ms_mixed * 1e-3), "unit": UNIT, "ms_per_step": ms_mixed,
+             "speedup_vs_fp64": ms / ms_mixed, "max_abs_err_vs_fp64": float(err.max()),
+             "max_rel_err_vs_fp64": float((err / ref.abs().clamp_min(1e-8)).max()),
+             "skip_bound": MIXED_SKIP, "fp32_bound": MIXED_FP32}
+    del ref, err
+
     # per-phase device times (events on the same stream), a separate pass of the same call
     db.set_profiling(True)
     ph = np.zeros(3)
@@ -285,7 +309,7 @@ def main():
                              f"{compact_bytes / 1e6:.0f} MB compact store)"},
             "phases_ms": {"work_list": ph[0], "class_kernels": ph[1], "expand": ph[2]},
             "roofline": roof, "roofline_kernels": [roof_compute, roof_expand],
-            "e2e": e2e, "clocks": clk.summary(),
+            "e2e": e2e, "clocks": clk.summary(), "mixed": mixed,
             "gpu_launches": None}
     # our kernels per step: work-list build + one per class block + expansion
     import gbasis_b200._engine as eng  # noqa: F401

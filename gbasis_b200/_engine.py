@@ -28,6 +28,7 @@ EXPORTED_SYMBOLS = (
     "gbx_lincomb", "gbx_eri_coulomb_j", "gbx_last_counts", "gbx_last_error", "gbx_fp64_peak",
     "gbx_set_profiling", "gbx_phase_times", "gbx_eri_full_noalloc",
     "gbx_num_blocks", "gbx_block_info", "gbx_set_team", "gbx_block_times",
+    "gbx_eri_full_mixed", "gbx_eri_unique",
 )
 
 
@@ -80,6 +81,8 @@ def lib():
                                ctypes.POINTER(_I64)],
             "gbx_set_team": [_P, _I, _I],
             "gbx_block_times": [_P, _P, _I],
+            "gbx_eri_full_mixed": [_P, _I, _D, _D, _P, _P],
+            "gbx_eri_unique": [_P, _D, _D, _P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -258,10 +261,21 @@ class DeviceBasis:
                                       stream), "gbx_eri_full_host")
         return out
 
-    def full_device(self, out_ptr, notation="chemist", schwarz_threshold=0.0, stream=None):
+    def full_device(self, out_ptr, notation="chemist", schwarz_threshold=0.0, stream=None,
+                    mixed=None):
+        """Full tensor into device memory.  ``mixed=(skip, fp32)`` selects the mixed form."""
         code = GBX_PHYSICIST if notation == "physicist" else GBX_CHEMIST
+        if mixed is not None:
+            check(lib().gbx_eri_full_mixed(self.handle, code, float(mixed[0]), float(mixed[1]),
+                                           ctypes.c_void_p(out_ptr), stream), "gbx_eri_full_mixed")
+            return
         check(lib().gbx_eri_full(self.handle, code, float(schwarz_threshold),
                                  ctypes.c_void_p(out_ptr), stream), "gbx_eri_full")
+
+    def unique(self, mixed=(0.0, 0.0), stream=None):
+        """Unique quartets into the engine's compact store (no expansion)."""
+        check(lib().gbx_eri_unique(self.handle, float(mixed[0]), float(mixed[1]), stream),
+              "gbx_eri_unique")
 
     def schwarz_bounds(self):
         ns = len(self.packed["angmom"])

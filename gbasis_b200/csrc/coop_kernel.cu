@@ -146,7 +146,7 @@ __global__ void eri_coop(const CoopArgs A) {
   const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
   for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + wib; w < count; w += nwarps) {
-    const int2 pq = a.work[a.work_off + w];
+    const int2 pq = a.work[a.reverse ? a.work_off + a.nwork - 1 - w : a.work_off + w];
     const PairDev P = a.pairs[pq.x];
     const PairDev Q = a.pairs[pq.y];
     for (int i = lane; i < NENF; i += 32) ACC[i] = 0.0;

@@ -163,8 +163,12 @@ __device__ __forceinline__ void coulomb_epilogue(const EriLaunch& a, int2 pq, co
   }
 }
 
-template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(kEriThreads) eri_block_fp64(const EriLaunch a) {
+// R = double: the FP64 form.  R = float: the mixed form's FP32 path — Boys values and the
+// geometric factors are formed in FP64 and rounded, the vertical and transfer recursions run
+// in FP32, and each primitive quartet's [e0|f0] is added to FP64 accumulators; the
+// horizontal recursion, transforms and stores stay FP64.
+template <int LA, int LB, int LC, int LD, typename R>
+__global__ void __launch_bounds__(kEriThreads) eri_block(const EriLaunch a) {
   using C = gen::Cls<LA, LB, LC, LD>;
   constexpr int L = C::L;
   constexpr int NCA = ncart(LA), NCB = ncart(LB), NCC = ncart(LC), NCD = ncart(LD);
@@ -187,7 +191,8 @@ __global__ void __launch_bounds__(kEriThreads) eri_block_fp64(const EriLaunch a)
   for (long long wb = gwarp * per_warp; wb < count; wb += nwarps * per_warp) {
     const long long w = wb + lane / team;
     const bool valid = w < count;
-    const int2 pq = valid ? a.work[a.work_off + w] : make_int2(0, 0);
+    const int2 pq = valid ? a.work[a.reverse ? a.work_off + a.nwork - 1 - w : a.work_off + w]
+                          : make_int2(0, 0);
     const PairDev P = a.pairs[pq.x];
     const PairDev Q = a.pairs[pq.y];
     double acc[C::NE * C::NF];
@@ -213,9 +218,24 @@ __global__ void __launch_bounds__(kEriThreads) eri_block_fp64(const EriLaunch a)
         for (int m = 0; m <= L; ++m) F[m] *= pref;
         const double ze = bp.zeta * kp.izeta;
         const double o2e = 0.5 * kp.izeta;
-        C::template prim<double>(F, bp.Xx, bp.Xy, bp.Xz, -rz * PQx, -rz * PQy, -rz * PQz, o2z,
-                                 rz, fma(ze, bp.Xx, kp.Xx), fma(ze, bp.Xy, kp.Xy),
-                                 fma(ze, bp.Xz, kp.Xz), ze, o2e, acc);
+        if constexpr (sizeof(R) == sizeof(double)) {
+          C::template prim<double>(F, bp.Xx, bp.Xy, bp.Xz, -rz * PQx, -rz * PQy, -rz * PQz,
+                                   o2z, rz, fma(ze, bp.Xx, kp.Xx), fma(ze, bp.Xy, kp.Xy),
+                                   fma(ze, bp.Xz, kp.Xz), ze, o2e, acc);
+        } else {
+          float F32[L + 1], a32[C::NE * C::NF];
+#pragma unroll
+          for (int m = 0; m <= L; ++m) F32[m] = (float)F[m];
+#pragma unroll
+          for (int i = 0; i < C::NE * C::NF; ++i) a32[i] = 0.0f;
+          C::template prim<float>(F32, (float)bp.Xx, (float)bp.Xy, (float)bp.Xz,
+                                  (float)(-rz * PQx), (float)(-rz * PQy), (float)(-rz * PQz),
+                                  (float)o2z, (float)rz, (float)fma(ze, bp.Xx, kp.Xx),
+                                  (float)fma(ze, bp.Xy, kp.Xy), (float)fma(ze, bp.Xz, kp.Xz),
+                                  (float)ze, (float)o2e, a32);
+#pragma unroll
+          for (int i = 0; i < C::NE * C::NF; ++i) acc[i] += (double)a32[i];
+        }
       }
       jq += team;
       while (jq >= Q.nprim) {

@@ -81,6 +81,8 @@ struct EriLaunch {
   long long base, ncols;
   int mode;                 // 0 = write block, 1 = Schwarz diagonal (max |.| -> qout)
   int team;                 // lanes per quartet in the register kernel (1..32, power of two)
+  int fp32;                 // register kernel: 1 = FP32 recursions (mixed form)
+  int reverse;              // quartet w is work[work_off + nwork - 1 - w] (FP32 list)
   // mode 2 (Coulomb matrix): J[a][b] += sum_cd (ab|cd) D[c][d] over the unique quartets
   const double* D;          // nbf x nbf, symmetric
   double* J;                // nbf x nbf, accumulated with atomics

@@ -416,7 +416,8 @@ def emit_sources(outdir, lmax):
                  "namespace gbx {",
                  "template <int LA, int LB, int LC, int LD>",
                  "int launch_t(const EriLaunch& a, int grid, cudaStream_t st) {",
-                 "  eri_block_fp64<LA, LB, LC, LD><<<grid, kEriThreads, 0, st>>>(a);",
+                 "  if (a.fp32) eri_block<LA, LB, LC, LD, float><<<grid, kEriThreads, 0, st>>>(a);",
+                 "  else eri_block<LA, LB, LC, LD, double><<<grid, kEriThreads, 0, st>>>(a);",
                  '  return cuda_status(cudaGetLastError(), "eri class kernel launch");',
                  "}"]
         for c in mine:

@@ -96,11 +96,11 @@ __global__ void build_work_range(const BuildBlock B, long long start, long long 
 
 __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* __restrict__ bb,
                            const double* __restrict__ qs, double tau, int2* __restrict__ work,
-                           int* __restrict__ counts) {
+                           int* __restrict__ counts, const MixedParams mp) {
   const int2 cm = cta_map[blockIdx.x];
   const BuildBlock B = bb[cm.x];
   const long long t = (long long)cm.y + threadIdx.x;
-  bool pass = false;
+  bool pass = false, fp32 = false;
   int p = 0, q = 0;
   if (t < B.ncand) {
     long long pl, ql;
@@ -116,16 +116,27 @@ __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* _
     p = B.pb0 + (int)pl;
     q = B.pk0 + (int)ql;
     pass = (tau <= 0.0) || (qs[p] * qs[q] >= tau);
+    if (mp.counts32) {
+      // mixed form: bound of the final values (Schwarz bound times the largest output scale
+      // of each shell) decides skip (< skip), FP32 (< fp32) or FP64
+      const double bnd = mp.qm[p] * mp.qm[q];
+      if (bnd < mp.skip) pass = false;
+      fp32 = pass && bnd < mp.fp32;
+    }
   }
-  const unsigned mask = __ballot_sync(0xffffffffu, pass);
+  const bool p64 = pass && !fp32;
+  const unsigned mask = __ballot_sync(0xffffffffu, p64);
+  const unsigned mask32 = __ballot_sync(0xffffffffu, fp32);
   const int lane = threadIdx.x & 31;
-  int base = 0;
+  int base = 0, base32 = 0;
   if (lane == 0 && mask) base = atomicAdd(&counts[B.blk], __popc(mask));
+  if (lane == 0 && mask32) base32 = atomicAdd(&mp.counts32[B.blk], __popc(mask32));
   base = __shfl_sync(0xffffffffu, base, 0);
-  if (pass) {
-    const int rank = __popc(mask & ((1u << lane) - 1u));
-    work[B.work_off + base + rank] = make_int2(p, q);
-  }
+  base32 = __shfl_sync(0xffffffffu, base32, 0);
+  const unsigned below = (1u << lane) - 1u;
+  if (p64) work[B.work_off + base + __popc(mask & below)] = make_int2(p, q);
+  if (fp32)  // FP32 quartets fill the block's slots from the end
+    work[B.work_off + B.ncand - 1 - (base32 + __popc(mask32 & below))] = make_int2(p, q);
 }
 
 // ------------------------------------------------------------------- K6
@@ -367,25 +378,44 @@ int ensure_schwarz(Basis& B, cudaStream_t st) {
   }
   GBX_CUDA(cudaMemcpy(B.d_qscreen, B.h_q.data(), np * sizeof(double), cudaMemcpyHostToDevice),
            "upload screening bounds");
+  // bounds of the final values for the mixed form: segmented-pair bound times the largest
+  // output scale (norm_cont x component norm or sign) of each of its two shells
+  std::vector<double> smax(n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int c = 0; c < kMaxCart; ++c) smax[i] = std::max(smax[i], std::fabs(B.shells[i].scl[c]));
+  std::vector<double> qm(np);
+  for (int p = 0; p < np; ++p) qm[p] = q[p] * smax[B.pairs[p].shA] * smax[B.pairs[p].shB];
+  if (!B.d_qmixed) {
+    const int s2 = B.alloc((void**)&B.d_qmixed, np * sizeof(double), "cudaMalloc(qmixed)");
+    if (s2) return s2;
+  }
+  GBX_CUDA(cudaMemcpy(B.d_qmixed, qm.data(), np * sizeof(double), cudaMemcpyHostToDevice),
+           "upload mixed bounds");
   B.schwarz_ready = true;
   return GBX_OK;
 }
 
-int run_compact(Basis& B, double tau, cudaStream_t st) {
+int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32) {
   int s;
-  if (tau > 0.0 && (s = ensure_schwarz(B, st))) return s;
+  const bool mixed = skip > 0.0 || fp32 > 0.0;
+  if ((tau > 0.0 || mixed) && (s = ensure_schwarz(B, st))) return s;
   if ((s = ensure_full_work(B))) return s;
   if ((s = B.ensure_scratch(B.compact_elems, 0))) return s;
   const int nblk = (int)B.blocks.size();
+  if (mixed && !B.d_counts32) {
+    if ((s = B.alloc((void**)&B.d_counts32, nblk * sizeof(int), "cudaMalloc(counts32)"))) return s;
+  }
   GBX_CUDA(cudaMemsetAsync(B.d_counts, 0, nblk * sizeof(int), st), "clear counts");
-  if (tau > 0.0) {
+  if (mixed) GBX_CUDA(cudaMemsetAsync(B.d_counts32, 0, nblk * sizeof(int), st), "clear counts");
+  if (tau > 0.0 || skip > 0.0) {
     // screened-out quartets are zero in the output: clear the store first
     GBX_CUDA(cudaMemsetAsync(B.d_compact, 0, B.compact_elems * sizeof(double), st),
              "clear compact store");
   }
+  const MixedParams mp{B.d_qmixed, skip, fp32, mixed ? B.d_counts32 : nullptr};
   if (B.profiling) cudaEventRecord(B.ev[0], st);
   build_work<<<B.n_cta_build, 256, 0, st>>>(B.d_cta_map, (const BuildBlock*)B.d_build_blocks,
-                                            B.d_qscreen, tau, B.d_work, B.d_counts);
+                                            B.d_qscreen, tau, B.d_work, B.d_counts, mp);
   GBX_CUDA(cudaGetLastError(), "build_work launch");
   if (B.profiling) cudaEventRecord(B.ev[1], st);
   const int nsm = num_sms(B.device);
@@ -427,6 +457,12 @@ int run_compact(Basis& B, double tau, cudaStream_t st) {
         (int)std::max<long long>(1, std::min<long long>((h.ncand * h.team + 127) / 128, (long long)nsm * 8));
     if (per_block) cudaEventRecord(B.blk_ev[i], st);
     if ((s = launch_class(la, lb, lc, ld, a, grid, bs))) return s;
+    if (mixed) {  // the block's FP32 list (the cooperative kernel runs it in FP64)
+      a.work_count = B.d_counts32 + k;
+      a.reverse = 1;
+      a.fp32 = 1;
+      if ((s = launch_class(la, lb, lc, ld, a, grid, bs))) return s;
+    }
   }
   if (per_block) cudaEventRecord(B.blk_ev[nblk], st);
   if (nstreams) {
@@ -487,8 +523,9 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
   return GBX_OK;
 }
 
-int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st) {
-  int s = run_compact(B, tau, st);
+int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, double skip,
+             double fp32) {
+  int s = run_compact(B, tau, st, skip, fp32);
   if (s) return s;
   ExpandArgs e;
   e.n = B.nbf;

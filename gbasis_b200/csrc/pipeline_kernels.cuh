@@ -29,9 +29,16 @@ __global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,
                                 const ShellDev* __restrict__ shells,
                                 const double* __restrict__ exps, const double* __restrict__ coefs,
                                 PrimPair* __restrict__ prims);
+// Mixed form of the work-list build (counts32 == nullptr: FP64 only, nothing skipped).
+struct MixedParams {
+  const double* qm;  // per pair: Schwarz bound x largest output scale of its two shells
+  double skip, fp32;
+  int* counts32;
+};
+
 __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* __restrict__ bb,
                            const double* __restrict__ qs, double tau, int2* __restrict__ work,
-                           int* __restrict__ counts);
+                           int* __restrict__ counts, const MixedParams mp);
 __global__ void expand_full(const ExpandArgs e);
 __global__ void build_work_range(const BuildBlock B, long long start, long long len,
                                  const double* __restrict__ qs, double tau,

@@ -389,6 +389,27 @@ int gbx_eri_full(gbx_basis* b, int notation, double tau, double* out, void* stre
   return run_full(B, notation, tau, out, (cudaStream_t)stream);
 }
 
+int gbx_eri_full_mixed(gbx_basis* b, int notation, double skip, double fp32, double* out,
+                       void* stream) {
+  if (!b || !out) return set_error(GBX_ERR_INVALID, "gbx_eri_full_mixed: null argument");
+  if (notation != GBX_CHEMIST && notation != GBX_PHYSICIST)
+    return set_error(GBX_ERR_INVALID, "notation must be GBX_CHEMIST or GBX_PHYSICIST");
+  if (!(skip >= 0.0) || !(fp32 >= 0.0))
+    return set_error(GBX_ERR_INVALID, "thresholds must be >= 0");
+  Basis& B = *b->impl;
+  DeviceGuard g(B.device);
+  return run_full(B, notation, 0.0, out, (cudaStream_t)stream, skip, fp32);
+}
+
+int gbx_eri_unique(gbx_basis* b, double skip, double fp32, void* stream) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_eri_unique: null basis");
+  if (!(skip >= 0.0) || !(fp32 >= 0.0))
+    return set_error(GBX_ERR_INVALID, "thresholds must be >= 0");
+  Basis& B = *b->impl;
+  DeviceGuard g(B.device);
+  return run_compact(B, 0.0, (cudaStream_t)stream, skip, fp32);
+}
+
 int gbx_eri_full_host(gbx_basis* b, int notation, double tau, double* out_host, void* stream) {
   if (!b || !out_host) return set_error(GBX_ERR_INVALID, "gbx_eri_full_host: null argument");
   Basis& B = *b->impl;

@@ -37,6 +37,8 @@ struct Basis {
   std::vector<long long> h_ftab;  // nbf*nbf function-pair keys of the expansion
   long long* d_ftab = nullptr;
   int2* d_jwork = nullptr;  // Coulomb chunk work list
+  int* d_counts32 = nullptr;   // mixed form: FP32 quartets per block
+  double* d_qmixed = nullptr;  // mixed form: per-pair bound of the final values
   std::vector<long long> class_first, class_count, class_funcs;
   std::vector<HostBlock> blocks;
   std::vector<BlockDev> block_table;  // kNumPairClasses^2, base = -1 when empty
@@ -90,8 +92,9 @@ int build_basis(Basis& B, int n, const int* angmom, const int* nprim, const doub
                 const int8_t* pos, const double* scl);
 void boys_host_table(double* h);
 int upload_basis(Basis& B);
-int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st);
-int run_compact(Basis& B, double tau, cudaStream_t st);
+int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, double skip = 0.0,
+             double fp32 = 0.0);
+int run_compact(Basis& B, double tau, cudaStream_t st, double skip = 0.0, double fp32 = 0.0);
 int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st);
 int ensure_schwarz(Basis& B, cudaStream_t st);
 int launch_class(int la, int lb, int lc, int ld, const EriLaunch& a, int grid, cudaStream_t st);

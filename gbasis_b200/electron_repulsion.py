@@ -64,6 +64,7 @@ class ElectronRepulsionIntegral:
 
     boys_func = staticmethod(_boys_host)
     _screen = 0.0
+    _mixed = None  # (skip, fp32) thresholds of the mixed-precision form
 
     def __init__(self, contractions):
         _check_contractions(contractions)
@@ -101,7 +102,20 @@ class ElectronRepulsionIntegral:
     def _full(self, coord_types, out=None, device=None):
         db = _engine.DeviceBasis(list(self.contractions), coord_types, device=device)
         try:
-            return db.full_host("chemist", self._screen, out=out)
+            if self._mixed is None:
+                return db.full_host("chemist", self._screen, out=out)
+            import ctypes
+            import torch
+            n = db.nbf
+            dev = torch.device("cuda", db.device)
+            buf = torch.empty(n ** 4, dtype=torch.float64, device=dev)
+            stream = torch.cuda.current_stream(dev).cuda_stream
+            db.full_device(buf.data_ptr(), "chemist", stream=ctypes.c_void_p(stream),
+                           mixed=self._mixed)
+            if out is None:
+                return buf.cpu().numpy().reshape(n, n, n, n)
+            torch.from_numpy(out.reshape(-1)).copy_(buf)
+            return out
         finally:
             db.close()
 
@@ -177,13 +191,27 @@ def _dispatch(cls_obj, basis, transform, coord_type, out, device):
     return cls_obj.construct_array_mix(types, out=out, device=device)
 
 
+MIXED_SKIP = 1e-11   # final-value Schwarz bound below which a quartet is zero (mixed form)
+MIXED_FP32 = 2e-6    # bound below which a quartet's recursions run in FP32 (mixed form)
+
+
 def electron_repulsion_integral(basis, transform=None, notation="physicist", *, coord_type=None,
-                                device=None, out=None):
+                                device=None, out=None, precision="fp64", mixed_skip=MIXED_SKIP,
+                                mixed_fp32=MIXED_FP32):
     """ERIs of ``basis`` (``electron_repulsion.py:214-281``): (K, K, K, K) float64, physicist
-    notation by default (a ``transpose(0, 2, 1, 3)`` view of the chemist array)."""
+    notation by default (a ``transpose(0, 2, 1, 3)`` view of the chemist array).
+
+    ``precision="mixed"`` selects the mixed form: quartets whose final-value Schwarz bound is
+    below ``mixed_skip`` are zero, those below ``mixed_fp32`` run their vertical and transfer
+    recursions in FP32."""
     if notation not in ["physicist", "chemist"]:
         raise ValueError("`notation` must be one of 'physicist' or 'chemist'")
-    array = _dispatch(ElectronRepulsionIntegral(basis), basis, transform, coord_type, out, device)
+    if precision not in ("fp64", "mixed"):
+        raise ValueError("`precision` must be 'fp64' or 'mixed'")
+    obj = ElectronRepulsionIntegral(basis)
+    if precision == "mixed":
+        obj._mixed = (float(mixed_skip), float(mixed_fp32))
+    array = _dispatch(obj, basis, transform, coord_type, out, device)
     if notation == "physicist":
         array = np.transpose(array, (0, 2, 1, 3))
     return array

@@ -86,7 +86,20 @@ int gbx_basis_stats(const gbx_basis* b, int64_t* n_quartets, int64_t* compact_by
  */
 int gbx_eri_full(gbx_basis* b, int notation, double schwarz_threshold, double* out,
                  void* stream);
-/* Same, into host memory (page-locked or pageable); synchronous. */
+/*
+ * Mixed-precision full tensor (no counterpart in the reference: gbasis computes in FP64
+ * only).  With B_q = Schwarz bound of the final values of quartet q (bound on blocks without
+ * norm_cont times the largest output scale of each shell): quartets with B_q < skip are
+ * zero, those with B_q < fp32 run the vertical/transfer recursions in FP32 (FP64
+ * accumulation over primitives, FP64 HRR and transforms), the rest in FP64.
+ */
+int gbx_eri_full_mixed(gbx_basis* b, int notation, double skip, double fp32, double* out,
+                       void* stream);
+/* Unique shell quartets only, into the engine's compact store (no N^4 expansion): the
+ * integral work of a full call, for bases whose full tensor does not fit in memory.
+ * skip = fp32 = 0 is the FP64 form. */
+int gbx_eri_unique(gbx_basis* b, double skip, double fp32, void* stream);
+/* Same as gbx_eri_full, into host memory (page-locked or pageable); synchronous. */
 int gbx_eri_full_host(gbx_basis* b, int notation, double schwarz_threshold, double* out_host,
                       void* stream);
 
