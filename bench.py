@@ -16,7 +16,8 @@ Cartesian; physicist notation as a view of the chemist array, as gbasis returns 
 
 ``--impl reference`` times that CPU implementation on all host cores instead and prints
 the same metric with ``"impl": "reference"``.  For N > 1 GPUs every rank computes the
-same workload (replicas; the north-star path runs on one GPU) and ``value`` aggregates.
+same workload (independent replicas: a full-tensor call needs no exchange between GPUs) and
+``value`` aggregates.
 """
 from __future__ import annotations
 
@@ -45,52 +46,71 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clock and clock-event (throttle) reasons of the benchmarked GPU, sampled every
+    ``period`` seconds through NVML from a background thread during the timed region (the
+    GPU is matched to the CUDA device by UUID).  Read-only: no clock or setting changes."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
-    def __init__(self, index):
-        self.index = index
-        self.p = None
+    def __init__(self, index, period=0.005):
+        self.index, self.period = index, period
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = None
+        self._thread = None
+
+    def _handle(self, nv):
+        import torch
+        want = str(torch.cuda.get_device_properties(self.index).uuid).lower()
+        for i in range(nv.nvmlDeviceGetCount()):
+            h = nv.nvmlDeviceGetHandleByIndex(i)
+            u = nv.nvmlDeviceGetUUID(h)
+            u = (u.decode() if isinstance(u, bytes) else u).lower()
+            if want and want in u:
+                return h
+        return nv.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _run(self, nv, h):
+        masks = [(name, getattr(nv, attr)) for name, attr in self.REASONS]
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for name, m in masks:
+                    if r & m:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(self.period)
 
     def __enter__(self):
+        import threading
         try:
-            self.p = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self._stop = threading.Event()
+            self._thread = threading.Thread(target=self._run, args=(nv, h), daemon=True)
+            self._thread.start()
+            t0 = time.perf_counter()
+            while not self.samples and time.perf_counter() - t0 < 1.0:
+                time.sleep(0.001)
         except Exception:
-            self.p = None
+            self._thread = None
         return self
 
     def __exit__(self, *a):
-        self.out = ""
-        if self.p is not None:
-            self.p.terminate()
-            try:
-                self.out, _ = self.p.communicate(timeout=5)
-            except Exception:
-                self.p.kill()
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in (self.out or "").splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = max(mx, float(f[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": mx or None, "reasons": sorted(reasons), "samples": len(sm)}
+        sm = self.samples
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(sm), "source": "NVML"}
 
 
 def cpu_baseline(shells, seconds=12.0, seed=0):

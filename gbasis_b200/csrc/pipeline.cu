@@ -200,6 +200,102 @@ __global__ void __launch_bounds__(256) expand_full(const ExpandArgs e) {
   }
 }
 
+// Row-staged expansion.  The unique integrals form a symmetric matrix M over pair functions
+// (class-major numbering); the compact store holds its class blocks (X, Y), X >= Y, and in a
+// diagonal block (X, X) the entries whose bra pair has the larger local index.  A CTA takes
+// pair functions r = blockIdx.x, blockIdx.x + gridDim.x, ...: it gathers row r of M into
+// shared memory (a contiguous row of each block (X, Y), a column of each block (Y, X)), then
+// writes the one or two N^2 planes of the output that row r fills — out[x, y, :, :] (chemist)
+// or out[x, :, y, :] (physicist) for the ordered function pairs (x, y) of r — with streaming
+// stores, each element gathered from shared memory through gtab.  CTAs in flight hold
+// consecutive rows, so the strided column reads of one block hit the same L2 sectors and the
+// compact store crosses HBM about once; the output is written once.
+// Row r of M (class X, row rho within the class, local pair index lr) into shared memory.
+__device__ __forceinline__ void stage_row(const ExpandArgs& e, long long r, int lr,
+                                          double* __restrict__ s_row) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  int X = 0;
+  while (r >= e.pf_first[X + 1]) ++X;
+  const long long rho = r - e.pf_first[X];
+  for (int Y = 0; Y < kNumPairClasses; ++Y) {
+    const long long y0 = e.pf_first[Y], ny = e.pf_first[Y + 1] - y0;
+    if (ny == 0) continue;
+    if (X > Y) {
+      const BlockDev b = e.blocks[X * kNumPairClasses + Y];
+      const double* __restrict__ src = e.compact + b.base + rho * b.ncols;
+      for (long long j = tid; j < ny; j += nt) s_row[y0 + j] = __ldg(src + j);
+    } else if (X < Y) {
+      const BlockDev b = e.blocks[Y * kNumPairClasses + X];
+      const double* __restrict__ src = e.compact + b.base + rho;
+      for (long long j = tid; j < ny; j += nt) s_row[y0 + j] = __ldg(src + j * b.ncols);
+    } else {
+      const BlockDev b = e.blocks[X * kNumPairClasses + X];
+      const double* __restrict__ blk = e.compact + b.base;
+      for (long long j = tid; j < ny; j += nt) {
+        const int lj = __ldg(&e.rowinfo[y0 + j].w);
+        s_row[y0 + j] = __ldg(lj <= lr ? blk + rho * b.ncols + j : blk + j * b.ncols + rho);
+      }
+    }
+  }
+}
+
+// One N^2 plane from the staged row: dst[c*cs + d] = M[r, gtab[c, d]], cs = N (chemist plane
+// out[x, y, :, :]) or N^2 (physicist out[x, :, y, :]).
+__device__ __forceinline__ void write_plane(const ExpandArgs& e, const double* __restrict__ s_row,
+                                            double* __restrict__ dst, bool phys) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const long long n = e.n, n2 = n * n;
+  if (!phys) {
+    for (long long t = tid; t < n2; t += nt) __stcs(dst + t, s_row[__ldg(e.gtab + t)]);
+  } else {
+    const unsigned un = (unsigned)n;
+    for (unsigned t = tid; t < (unsigned)n2; t += nt) {
+      const unsigned c = t / un, d = t - c * un;
+      __stcs(dst + (long long)c * n2 + d, s_row[__ldg(e.gtab + t)]);
+    }
+  }
+}
+
+__device__ __forceinline__ double* plane_ptr(const ExpandArgs& e, double* base, long long x,
+                                             long long y, bool phys) {
+  const long long n = e.n, n2 = n * n;
+  return phys ? base + x * n * n2 + y * n : base + (x * n + y) * n2;
+}
+
+__global__ void __launch_bounds__(512) expand_rows(const ExpandArgs e) {
+  extern __shared__ double s_row[];
+  const bool phys = e.notation == GBX_PHYSICIST;
+  for (long long r = blockIdx.x; r < e.npf; r += gridDim.x) {
+    const int4 ri = __ldg(e.rowinfo + r);
+    if (ri.x < 0) continue;  // no ordered pair maps here (cannot happen for a built basis)
+    __syncthreads();  // the previous row's planes are written
+    stage_row(e, r, ri.w, s_row);
+    __syncthreads();
+    write_plane(e, s_row, plane_ptr(e, e.out, ri.x, ri.y, phys), phys);
+    if (ri.z) write_plane(e, s_row, plane_ptr(e, e.out, ri.y, ri.x, phys), phys);
+  }
+}
+
+// Slab form of the row-staged expansion: the planes of x in [x0, x1) only — the contiguous
+// range out[x0 * N^3, x1 * N^3) — into dst (which holds that range), one plane per ordered
+// pair (x, y).  Used to stream the tensor to host memory slab by slab.
+__global__ void __launch_bounds__(512) expand_slab(const ExpandArgs e, long long x0, long long x1,
+                                                   double* __restrict__ dst) {
+  extern __shared__ double s_row[];
+  const bool phys = e.notation == GBX_PHYSICIST;
+  const long long n = e.n;
+  const long long np = (x1 - x0) * n;
+  for (long long q = blockIdx.x; q < np; q += gridDim.x) {
+    const long long x = x0 + q / n, y = q % n;
+    const long long r = __ldg(e.gtab + x * n + y);
+    const int lr = __ldg(&e.rowinfo[r].w);
+    __syncthreads();
+    stage_row(e, r, lr, s_row);
+    __syncthreads();
+    write_plane(e, s_row, plane_ptr(e, dst, x - x0, y, phys), phys);
+  }
+}
+
 // ------------------------------------------------------------------- host side
 static int num_sms(int device) {
   int v = 0;
@@ -266,6 +362,15 @@ int upload_basis(Basis& B) {
     return s;
   GBX_CUDA(cudaMemcpy(B.d_ftab, B.h_ftab.data(), B.h_ftab.size() * sizeof(long long),
                       cudaMemcpyHostToDevice), "upload ftab");
+  if ((s = B.alloc((void**)&B.d_gtab, B.h_gtab.size() * sizeof(int), "cudaMalloc(gtab)")))
+    return s;
+  GBX_CUDA(cudaMemcpy(B.d_gtab, B.h_gtab.data(), B.h_gtab.size() * sizeof(int),
+                      cudaMemcpyHostToDevice), "upload gtab");
+  if ((s = B.alloc((void**)&B.d_rowinfo, B.h_rowinfo.size() * sizeof(int4),
+                   "cudaMalloc(rowinfo)")))
+    return s;
+  GBX_CUDA(cudaMemcpy(B.d_rowinfo, B.h_rowinfo.data(), B.h_rowinfo.size() * sizeof(int4),
+                      cudaMemcpyHostToDevice), "upload rowinfo");
   if ((s = B.alloc((void**)&B.d_q, np * sizeof(double), "cudaMalloc(q)"))) return s;
   if ((s = B.alloc((void**)&B.d_qscreen, np * sizeof(double), "cudaMalloc(qscreen)"))) return s;
   if ((s = boys_table(B.device, &B.d_boys))) return s;
@@ -523,10 +628,7 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
   return GBX_OK;
 }
 
-int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, double skip,
-             double fp32) {
-  int s = run_compact(B, tau, st, skip, fp32);
-  if (s) return s;
+static ExpandArgs expand_args(const Basis& B, int notation, double* out) {
   ExpandArgs e;
   e.n = B.nbf;
   e.nsh = (int)B.shells.size();
@@ -539,12 +641,119 @@ int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, d
   e.compact = B.d_compact;
   e.out = out;
   e.ftab = B.d_ftab;
-  const long long rows = (long long)B.nbf * B.nbf * B.nbf;
-  const int grid = (int)std::max<long long>(1, std::min<long long>((rows + 7) / 8,
-                                                                    (long long)num_sms(B.device) * 16));
+  e.gtab = B.d_gtab;
+  e.rowinfo = B.d_rowinfo;
+  e.npf = B.pf_first[kNumPairClasses];
+  for (int c = 0; c <= kNumPairClasses; ++c) e.pf_first[c] = B.pf_first[c];
+  return e;
+}
+
+// CTAs per SM of a row-staged expansion kernel with one M row in shared memory (0 when the
+// row does not fit).
+template <typename K>
+static int row_kernel_fit(const Basis& B, K kernel, size_t row_bytes, int* per_sm) {
+  *per_sm = 0;
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, B.device);
+  if (row_bytes > (size_t)optin) return GBX_OK;
+  if (row_bytes > 48 * 1024)
+    GBX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)row_bytes), "expansion smem attribute");
+  GBX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kernel, 512, row_bytes),
+           "expansion occupancy");
+  return GBX_OK;
+}
+
+// Full tensor into host memory without an N^4 device buffer: after the class kernels, the
+// tensor is expanded slab by slab (x-ranges of out[x, ...], each a contiguous host range)
+// into kStageBuffers device staging slabs; each slab is copied out on a copy stream while
+// the next ones expand.  Host memory may be pageable or page-locked (page-locked copies run
+// asynchronously and overlap fully).  Synchronous.
+int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStream_t st) {
+  const long long n = B.nbf;
+  const size_t slab = (size_t)n * n * n;  // elements of one x
+  const size_t row_bytes = (size_t)B.pf_first[kNumPairClasses] * sizeof(double);
+  int per_sm = 0, s;
+  if ((s = row_kernel_fit(B, expand_slab, row_bytes, &per_sm))) return s;
+  if (per_sm == 0) {
+    // a pair-function row larger than shared memory: whole tensor on the device, one copy
+    if ((s = B.ensure_out((size_t)n * slab))) return s;
+    if ((s = run_full(B, notation, tau, B.d_out, st))) return s;
+    GBX_CUDA(cudaMemcpyAsync(out_host, B.d_out, (size_t)n * slab * sizeof(double),
+                             cudaMemcpyDeviceToHost, st), "copy tensor to host");
+    GBX_CUDA(cudaStreamSynchronize(st), "synchronize");
+    return GBX_OK;
+  }
+  const long long xs = std::max<long long>(1, (long long)(kStageBytes / (slab * sizeof(double))));
+  const size_t chunk = (size_t)std::min<long long>(xs, n) * slab;
+  if (B.stage_elems < chunk) {
+    if (B.d_stage) {
+      cudaFree(B.d_stage);
+      B.dev_allocs.erase(std::find(B.dev_allocs.begin(), B.dev_allocs.end(), (void*)B.d_stage));
+      B.d_stage = nullptr;
+      B.stage_elems = 0;
+    }
+    if ((s = B.alloc((void**)&B.d_stage, kStageBuffers * chunk * sizeof(double),
+                     "cudaMalloc(staging slabs)")))
+      return s;
+    B.stage_elems = chunk;
+  }
+  if (!B.copy_stream) {
+    GBX_CUDA(cudaStreamCreateWithFlags(&B.copy_stream, cudaStreamNonBlocking), "create stream");
+    for (int k = 0; k < kStageBuffers; ++k) {
+      GBX_CUDA(cudaEventCreateWithFlags(&B.stage_ready[k], cudaEventDisableTiming), "event");
+      GBX_CUDA(cudaEventCreateWithFlags(&B.stage_free[k], cudaEventDisableTiming), "event");
+    }
+  }
+  if ((s = run_compact(B, tau, st))) return s;
+  const ExpandArgs e = expand_args(B, notation, nullptr);
+  const int nsm = num_sms(B.device);
+  int i = 0;
+  for (long long x0 = 0; x0 < n; x0 += xs, ++i) {
+    const long long x1 = std::min(n, x0 + xs);
+    const int k = i % kStageBuffers;
+    double* buf = B.d_stage + (size_t)k * B.stage_elems;
+    if (i >= kStageBuffers) GBX_CUDA(cudaStreamWaitEvent(st, B.stage_free[k], 0), "wait slab");
+    const long long planes = (x1 - x0) * n;
+    const int grid = (int)std::max<long long>(1, std::min<long long>(planes, (long long)nsm * per_sm));
+    expand_slab<<<grid, 512, row_bytes, st>>>(e, x0, x1, buf);
+    GBX_CUDA(cudaGetLastError(), "expand_slab launch");
+    GBX_CUDA(cudaEventRecord(B.stage_ready[k], st), "record slab");
+    GBX_CUDA(cudaStreamWaitEvent(B.copy_stream, B.stage_ready[k], 0), "wait slab");
+    GBX_CUDA(cudaMemcpyAsync(out_host + (size_t)x0 * slab, buf,
+                             (size_t)(x1 - x0) * slab * sizeof(double), cudaMemcpyDeviceToHost,
+                             B.copy_stream),
+             "copy slab to host");
+    GBX_CUDA(cudaEventRecord(B.stage_free[k], B.copy_stream), "record slab copy");
+  }
+  GBX_CUDA(cudaStreamSynchronize(B.copy_stream), "synchronize copies");
+  GBX_CUDA(cudaStreamSynchronize(st), "synchronize");
+  return GBX_OK;
+}
+
+int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, double skip,
+             double fp32) {
+  int s = run_compact(B, tau, st, skip, fp32);
+  if (s) return s;
+  const ExpandArgs e = expand_args(B, notation, out);
   if (B.profiling) cudaEventRecord(B.ev[2], st);
-  expand_full<<<grid, 256, 0, st>>>(e);
-  GBX_CUDA(cudaGetLastError(), "expand_full launch");
+  const size_t row_bytes = (size_t)e.npf * sizeof(double);
+  int per_sm = 0;
+  if ((s = row_kernel_fit(B, expand_rows, row_bytes, &per_sm))) return s;
+  if (per_sm > 0) {
+    // one pair-function row of M in shared memory per CTA; persistent grid of the CTAs that
+    // fit on the SMs together
+    const int grid = (int)std::max<long long>(
+        1, std::min<long long>(e.npf, (long long)num_sms(B.device) * per_sm));
+    expand_rows<<<grid, 512, row_bytes, st>>>(e);
+    GBX_CUDA(cudaGetLastError(), "expand_rows launch");
+  } else {
+    const long long rows = (long long)B.nbf * B.nbf * B.nbf;
+    const int grid = (int)std::max<long long>(
+        1, std::min<long long>((rows + 7) / 8, (long long)num_sms(B.device) * 16));
+    expand_full<<<grid, 256, 0, st>>>(e);
+    GBX_CUDA(cudaGetLastError(), "expand_full launch");
+  }
   if (B.profiling) cudaEventRecord(B.ev[3], st);
   return GBX_OK;
 }

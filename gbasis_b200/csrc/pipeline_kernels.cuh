@@ -23,6 +23,11 @@ struct ExpandArgs {
   const double* compact;
   double* out;
   const long long* ftab;  // n*n function-pair keys (class, pair index in class, block row)
+  // row-staged form (expand_rows)
+  const int* gtab;        // n*n: pair function (class-major index) of each ordered pair
+  const int4* rowinfo;    // per pair function: (x, y, mirror, local pair index in class)
+  long long npf;
+  long long pf_first[kNumPairClasses + 1];
 };
 
 __global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,
@@ -40,6 +45,7 @@ __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* _
                            const double* __restrict__ qs, double tau, int2* __restrict__ work,
                            int* __restrict__ counts, const MixedParams mp);
 __global__ void expand_full(const ExpandArgs e);
+__global__ void expand_rows(const ExpandArgs e);
 __global__ void build_work_range(const BuildBlock B, long long start, long long len,
                                  const double* __restrict__ qs, double tau,
                                  int2* __restrict__ work, int* __restrict__ count);

@@ -114,6 +114,11 @@ Basis::~Basis() {
   for (cudaEvent_t& e : join)
     if (e) cudaEventDestroy(e);
   if (fork) cudaEventDestroy(fork);
+  for (cudaEvent_t& e : stage_ready)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t& e : stage_free)
+    if (e) cudaEventDestroy(e);
+  if (copy_stream) cudaStreamDestroy(copy_stream);
 }
 
 int Basis::alloc(void** p, size_t bytes, const char* what) {
@@ -135,6 +140,20 @@ int Basis::ensure_scratch(size_t compact_elems, size_t work_elems) {
     compact_cap = compact_elems;
   }
   (void)work_elems;
+  return GBX_OK;
+}
+
+int Basis::ensure_out(size_t elems) {
+  if (elems <= out_cap) return GBX_OK;
+  if (d_out) {
+    cudaFree(d_out);
+    dev_allocs.erase(std::find(dev_allocs.begin(), dev_allocs.end(), (void*)d_out));
+    d_out = nullptr;
+    out_cap = 0;
+  }
+  int s = alloc((void**)&d_out, elems * sizeof(double), "cudaMalloc(full tensor)");
+  if (s) return s;
+  out_cap = elems;
   return GBX_OK;
 }
 
@@ -279,6 +298,26 @@ int build_basis(Basis& B, int n, const int* angmom, const int* nprim, const doub
         B.h_ftab[(size_t)x * B.nbf + y] =
             ((long long)p.cls << 56) | ((long long)p.local << 32) | row;
       }
+    // row-staged expansion: global pair-function index (class-major), the ordered function
+    // pairs of each pair function and the pair each one belongs to
+    B.pf_first.assign(kNumPairClasses + 1, 0);
+    for (int c = 0; c < kNumPairClasses; ++c) B.pf_first[c + 1] = B.pf_first[c] + B.class_funcs[c];
+    const long long npf = B.pf_first[kNumPairClasses];
+    B.h_gtab.resize((size_t)B.nbf * B.nbf);
+    B.h_rowinfo.assign((size_t)npf, make_int4(-1, -1, 0, 0));
+    for (long long x = 0; x < B.nbf; ++x)
+      for (long long y = 0; y < B.nbf; ++y) {
+        const long long k = B.h_ftab[(size_t)x * B.nbf + y];
+        const int cls = (int)(k >> 56);
+        const long long g = B.pf_first[cls] + (k & 0xffffffffLL);
+        B.h_gtab[(size_t)x * B.nbf + y] = (int)g;
+        int4& ri = B.h_rowinfo[(size_t)g];
+        if (ri.x < 0) {
+          ri = make_int4((int)x, (int)y, 0, (int)((k >> 32) & 0xffffff));
+        } else if (ri.x == (int)y && ri.y == (int)x) {
+          ri.z = 1;  // (y, x) is the mirror of the stored ordered pair
+        }
+      }
   }
   // default lanes-per-quartet: about four primitive quartets per lane, fewer lanes when the
   // accumulator set (reduced across the team by shuffles) is large
@@ -412,26 +451,12 @@ int gbx_eri_unique(gbx_basis* b, double skip, double fp32, void* stream) {
 
 int gbx_eri_full_host(gbx_basis* b, int notation, double tau, double* out_host, void* stream) {
   if (!b || !out_host) return set_error(GBX_ERR_INVALID, "gbx_eri_full_host: null argument");
+  if (notation != GBX_CHEMIST && notation != GBX_PHYSICIST)
+    return set_error(GBX_ERR_INVALID, "notation must be GBX_CHEMIST or GBX_PHYSICIST");
+  if (!(tau >= 0.0)) return set_error(GBX_ERR_INVALID, "schwarz threshold must be >= 0");
   Basis& B = *b->impl;
   DeviceGuard g(B.device);
-  const size_t n4 = (size_t)B.nbf * B.nbf * B.nbf * B.nbf;
-  if (n4 > B.out_cap) {
-    if (B.d_out) {
-      cudaFree(B.d_out);
-      B.dev_allocs.erase(std::find(B.dev_allocs.begin(), B.dev_allocs.end(), (void*)B.d_out));
-      B.d_out = nullptr;
-    }
-    int s = B.alloc((void**)&B.d_out, n4 * sizeof(double), "cudaMalloc(full tensor)");
-    if (s) return s;
-    B.out_cap = n4;
-  }
-  cudaStream_t st = (cudaStream_t)stream;
-  int s = gbx_eri_full(b, notation, tau, B.d_out, stream);
-  if (s) return s;
-  GBX_CUDA(cudaMemcpyAsync(out_host, B.d_out, n4 * sizeof(double), cudaMemcpyDeviceToHost, st),
-           "copy tensor to host");
-  GBX_CUDA(cudaStreamSynchronize(st), "synchronize");
-  return GBX_OK;
+  return run_full_host(B, notation, tau, out_host, (cudaStream_t)stream);
 }
 
 int gbx_schwarz_bounds(gbx_basis* b, double* q_host) {

@@ -12,6 +12,8 @@ namespace gbx {
 
 constexpr int kAuxStreams = 6;
 constexpr long long kCoulombChunk = 1LL << 24;  // quartet candidates per Coulomb chunk
+constexpr int kStageBuffers = 3;                // host-output staging slabs in flight
+constexpr size_t kStageBytes = 64ull << 20;     // target bytes of one staging slab
 
 int boys_table(int device, const double** out);
 int compiled_lmax();
@@ -36,6 +38,14 @@ struct Basis {
   std::vector<int> group;    // original (generalized) shell of each segmented shell
   std::vector<long long> h_ftab;  // nbf*nbf function-pair keys of the expansion
   long long* d_ftab = nullptr;
+  // row-staged expansion: pair functions numbered class-major (pf_first[c] = first of class
+  // c), gtab[x*nbf+y] = pair function of the ordered function pair (x, y), rowinfo[g] =
+  // (x, y, 1 if (y, x) is the same pair function, local pair index in its class)
+  std::vector<long long> pf_first;
+  std::vector<int> h_gtab;
+  std::vector<int4> h_rowinfo;
+  int* d_gtab = nullptr;
+  int4* d_rowinfo = nullptr;
   int2* d_jwork = nullptr;  // Coulomb chunk work list
   int* d_counts32 = nullptr;   // mixed form: FP32 quartets per block
   double* d_qmixed = nullptr;  // mixed form: per-pair bound of the final values
@@ -80,11 +90,18 @@ struct Basis {
   std::vector<cudaStream_t> aux;    // concurrent class-block streams
   std::vector<cudaEvent_t> join;
   cudaEvent_t fork = nullptr;
+  // host-output streaming: staging slabs on the device, copied out on their own stream
+  double* d_stage = nullptr;
+  size_t stage_elems = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t stage_ready[kStageBuffers] = {};
+  cudaEvent_t stage_free[kStageBuffers] = {};
   std::vector<void*> dev_allocs;
 
   ~Basis();
   int alloc(void** p, size_t bytes, const char* what);
   int ensure_scratch(size_t compact_elems, size_t work_elems);
+  int ensure_out(size_t elems);
 };
 
 int build_basis(Basis& B, int n, const int* angmom, const int* nprim, const double* center,
@@ -94,6 +111,7 @@ void boys_host_table(double* h);
 int upload_basis(Basis& B);
 int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, double skip = 0.0,
              double fp32 = 0.0);
+int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStream_t st);
 int run_compact(Basis& B, double tau, cudaStream_t st, double skip = 0.0, double fp32 = 0.0);
 int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st);
 int ensure_schwarz(Basis& B, cudaStream_t st);

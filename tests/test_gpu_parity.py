@@ -176,6 +176,25 @@ def test_medium8_full_size_sampled_parity_and_symmetry():
     assert np.all(v * v <= D2[a, b] * D2[c, d] * (1 + 1e-10) + 1e-24)
 
 
+@pytest.mark.parametrize("notation", ["chemist", "physicist"])
+def test_streamed_host_tensor_equals_device_tensor(notation):
+    """Host output is expanded slab by slab (30 staging slabs for N = 120) and copied out
+    while later slabs expand; it must equal the device-resident tensor bit for bit."""
+    import torch
+    shells = make_workload("medium8")
+    db = _engine.DeviceBasis(shells)
+    n = db.nbf
+    dev = torch.empty(n ** 4, dtype=torch.float64, device="cuda")
+    db.full_device(dev.data_ptr(), notation)
+    torch.cuda.synchronize()
+    host = db.full_host(notation)
+    np.testing.assert_array_equal(host.reshape(-1), dev.cpu().numpy())
+    pinned = torch.empty(n ** 4, dtype=torch.float64, pin_memory=True).numpy().reshape((n,) * 4)
+    db.full_host(notation, out=pinned)
+    np.testing.assert_array_equal(pinned, host)
+    db.close()
+
+
 def test_errors_match_reference_behaviour():
     shells = make_workload("tiny4")
     with pytest.raises(ValueError):
