@@ -29,6 +29,8 @@ EXPORTED_SYMBOLS = (
     "gbx_set_profiling", "gbx_phase_times", "gbx_eri_full_noalloc",
     "gbx_num_blocks", "gbx_block_info", "gbx_set_team", "gbx_block_times",
     "gbx_eri_full_mixed", "gbx_eri_unique",
+    "gbx_batch_create", "gbx_batch_destroy", "gbx_batch_info", "gbx_batch_run",
+    "gbx_batch_set_graph",
 )
 
 
@@ -83,6 +85,12 @@ def lib():
             "gbx_block_times": [_P, _P, _I],
             "gbx_eri_full_mixed": [_P, _I, _D, _D, _P, _P],
             "gbx_eri_unique": [_P, _D, _D, _P],
+            "gbx_batch_create": [ctypes.POINTER(_P), _I, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                 _P, _I],
+            "gbx_batch_destroy": [_P],
+            "gbx_batch_info": [_P, _P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
+            "gbx_batch_run": [_P, _I, _P, _P],
+            "gbx_batch_set_graph": [_P, _I],
         }
         for name, args in sig.items():
             f = getattr(L, name)

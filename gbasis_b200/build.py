@@ -41,7 +41,7 @@ def sources(lmax):
     gen = gen_eri.emit_sources(GEN, lmax)
     return [os.path.join(GEN, g) for g in gen] + [
         os.path.join(CSRC, f) for f in ("runtime.cu", "pipeline.cu", "extras.cu", "noalloc.cu",
-                                        "coop_kernel.cu")]
+                                        "coop_kernel.cu", "batch.cu")]
 
 
 KERNEL_DEPS = ("gbx_common.cuh", "eri_kernels.cuh", "errors.h", "_gen/eri_gen.cuh")

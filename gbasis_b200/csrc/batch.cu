@@ -1,0 +1,427 @@
+// Batched full tensors of many molecules, replayed as one CUDA graph.
+//
+// A batch merges its molecules' shells, pairs and primitive pairs into single device arrays
+// (each pair records its molecule), and for every block type (bra pair class, ket pair
+// class) concatenates the unique quartets of all molecules into one work list: one class
+// kernel launch per block type covers the whole batch, writing each quartet into its own
+// molecule's compact store (per-molecule block base and column count, looked up by the bra
+// pair's molecule).  One batched row-staged expansion then writes every molecule's N^4
+// tensor.  The work lists are static (full tensors screen nothing), so the launches — class
+// kernels spread over auxiliary streams, joined, then the expansion — are captured once into
+// a CUDA graph and replayed; output pointers and notation live in a device table that each
+// run updates before the replay.  No counterpart in gbasis (one molecule per call there).
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "gbx_eri.h"
+#include "gbx_common.cuh"
+#include "pipeline_kernels.cuh"
+#include "runtime.h"
+
+namespace gbx {
+
+#define GBX_CUDA(call, what)              \
+  do {                                    \
+    int _s = cuda_status((call), (what)); \
+    if (_s != GBX_OK) return _s;          \
+  } while (0)
+
+struct BatchType {
+  int cb, ck;
+  long long n = 0, work_off = 0;
+  double avg_prims = 1.0;
+  int team = 1;
+  long long* d_base = nullptr;   // per molecule: block base in the batch compact store
+  long long* d_ncols = nullptr;  // per molecule: pair functions of the ket class
+};
+
+struct Batch {
+  int device = 0;
+  int nmol = 0;
+  std::vector<std::unique_ptr<Basis>> mols;  // host tables of each molecule
+  std::vector<long long> compact_off;
+  std::vector<BatchType> types;
+  std::vector<int> order;  // block types, largest estimated cost first
+  ShellDev* d_shells = nullptr;
+  PairDev* d_pairs = nullptr;
+  PrimPair* d_prims = nullptr;
+  double* d_exps = nullptr;
+  double* d_coefs = nullptr;
+  const double* d_boys = nullptr;
+  int2* d_work = nullptr;
+  double* d_compact = nullptr;
+  int* d_gtab = nullptr;
+  int4* d_rowinfo = nullptr;
+  BlockDev* d_blocks = nullptr;
+  ExpandArgs* d_exp = nullptr;
+  long long* d_row_first = nullptr;
+  std::vector<ExpandArgs> h_exp;
+  long long total_rows = 0, n_quartets = 0, compact_elems = 0;
+  size_t max_row_bytes = 0;
+  cudaStream_t exec = nullptr;
+  std::vector<cudaStream_t> aux;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr, ev_in = nullptr, ev_out = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  bool use_graph = true;
+  bool exp_dirty = true;
+  std::vector<void*> allocs;
+
+  int alloc(void** p, size_t bytes, const char* what) {
+    if (bytes == 0) bytes = 16;
+    GBX_CUDA(cudaMalloc(p, bytes), what);
+    allocs.push_back(*p);
+    return GBX_OK;
+  }
+  template <typename T>
+  int upload(T** d, const std::vector<T>& h, const char* what) {
+    int s = alloc((void**)d, h.size() * sizeof(T), what);
+    if (s) return s;
+    GBX_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), what);
+    return GBX_OK;
+  }
+  ~Batch() {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void* p : allocs) cudaFree(p);
+    for (cudaStream_t s : aux) cudaStreamDestroy(s);
+    for (cudaEvent_t e : join) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+    if (exec) cudaStreamDestroy(exec);
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// Lanes per quartet of the register kernel: about four primitive quartets per lane, fewer
+// lanes when the accumulator set (reduced by shuffles) is large.
+static int default_team(int cb, int ck, double avg_prims) {
+  const int la = kPairClassL[cb][0], lb = kPairClassL[cb][1];
+  const int lc = kPairClassL[ck][0], ld = kPairClassL[ck][1];
+  int ne = 0, nf = 0;
+  for (int e = la; e <= la + lb; ++e) ne += ncart(e);
+  for (int f = lc; f <= lc + ld; ++f) nf += ncart(f);
+  const int cap = ne * nf > 100 ? 2 : (ne * nf > 40 ? 8 : 32);
+  int t = 1;
+  while (t < cap && avg_prims / (2 * t) >= 4.0) t *= 2;
+  return t;
+}
+
+static int build_batch(Batch& Bt, int n_mol, const int* mol_nshells, const int* angmom,
+                       const int* nprim, const double* center, const double* exps,
+                       const double* coefs, const int* nout, const int* sph, const int8_t* pos,
+                       const double* scl) {
+  Bt.nmol = n_mol;
+  std::vector<ShellDev> shells;
+  std::vector<PairDev> pairs;
+  std::vector<double> hexps, hcoefs;
+  std::vector<long long> pair_off(n_mol + 1, 0);
+  long long sh0 = 0, ex0 = 0, pp0 = 0, c0 = 0;
+  for (int m = 0; m < n_mol; ++m) {
+    const int ns = mol_nshells[m];
+    if (ns <= 0) return set_error(GBX_ERR_INVALID, "molecule %d has no shells", m);
+    long long nex = 0;
+    for (int s = 0; s < ns; ++s) nex += nprim[sh0 + s];
+    auto B = std::make_unique<Basis>();
+    B->device = Bt.device;
+    B->lmax_supported = compiled_lmax();
+    int s = build_basis(*B, ns, angmom + sh0, nprim + sh0, center + 3 * sh0, exps + ex0,
+                        coefs + ex0, nout + sh0, sph + sh0, pos + kMaxCart * sh0,
+                        scl + kMaxCart * sh0);
+    if (s) return set_error(s, "molecule %d: %s", m, gbx_last_error_str());
+    for (ShellDev d : B->shells) {
+      d.prim_off += (int)ex0;
+      shells.push_back(d);
+    }
+    for (PairDev p : B->pairs) {
+      p.shA += (int)sh0;
+      p.shB += (int)sh0;
+      p.prim_off += (int)pp0;
+      p.mol = m;
+      pairs.push_back(p);
+    }
+    hexps.insert(hexps.end(), exps + ex0, exps + ex0 + nex);
+    hcoefs.insert(hcoefs.end(), coefs + ex0, coefs + ex0 + nex);
+    pair_off[m + 1] = pair_off[m] + (long long)B->pairs.size();
+    Bt.compact_off.push_back(c0);
+    c0 += B->compact_elems;
+    sh0 += ns;
+    ex0 += nex;
+    pp0 += B->n_prim_pairs;
+    Bt.mols.push_back(std::move(B));
+  }
+  Bt.compact_elems = c0;
+  if (pp0 > (1LL << 31) - 1 || (long long)pairs.size() > (1LL << 31) - 1)
+    return set_error(GBX_ERR_UNSUPPORTED, "batch too large for 32-bit pair indices");
+
+  // block types: every molecule's quartets of (cb, ck), concatenated
+  std::vector<int2> work;
+  std::vector<std::vector<long long>> tbase, tcols;
+  for (int cb = 0; cb < kNumPairClasses; ++cb)
+    for (int ck = 0; ck <= cb; ++ck) {
+      BatchType T;
+      T.cb = cb;
+      T.ck = ck;
+      T.work_off = (long long)work.size();
+      std::vector<long long> base(n_mol, 0), cols(n_mol, 0);
+      double prim_sum = 0.0;
+      for (int m = 0; m < n_mol; ++m) {
+        const Basis& B = *Bt.mols[m];
+        const BlockDev& bd = B.block_table[(size_t)cb * kNumPairClasses + ck];
+        if (bd.base < 0) continue;
+        base[m] = Bt.compact_off[m] + bd.base;
+        cols[m] = bd.ncols;
+        const long long fb = B.class_first[cb], nb = B.class_count[cb];
+        const long long fk = B.class_first[ck], nk = B.class_count[ck];
+        for (long long pl = 0; pl < nb; ++pl) {
+          const long long qn = (cb == ck) ? pl + 1 : nk;
+          const int p = (int)(pair_off[m] + fb + pl);
+          for (long long ql = 0; ql < qn; ++ql) {
+            const int q = (int)(pair_off[m] + fk + ql);
+            work.push_back(make_int2(p, q));
+            prim_sum += (double)pairs[p].nprim * pairs[q].nprim;
+          }
+        }
+      }
+      T.n = (long long)work.size() - T.work_off;
+      if (T.n == 0) continue;
+      T.avg_prims = prim_sum / (double)T.n;
+      T.team = default_team(cb, ck, T.avg_prims);
+      Bt.types.push_back(T);
+      tbase.push_back(std::move(base));
+      tcols.push_back(std::move(cols));
+    }
+  Bt.n_quartets = (long long)work.size();
+  std::vector<double> cost(Bt.types.size());
+  for (size_t k = 0; k < Bt.types.size(); ++k) {
+    const BatchType& T = Bt.types[k];
+    cost[k] = (double)T.n * (T.avg_prims + 4.0) * ncart(kPairClassL[T.cb][0]) *
+              ncart(kPairClassL[T.cb][1]) * ncart(kPairClassL[T.ck][0]) * ncart(kPairClassL[T.ck][1]);
+  }
+  Bt.order.resize(Bt.types.size());
+  for (size_t k = 0; k < Bt.order.size(); ++k) Bt.order[k] = (int)k;
+  std::stable_sort(Bt.order.begin(), Bt.order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+
+  // device arrays
+  DeviceGuardLite g(Bt.device);
+  int s;
+  if ((s = Bt.upload(&Bt.d_shells, shells, "upload batch shells"))) return s;
+  if ((s = Bt.upload(&Bt.d_pairs, pairs, "upload batch pairs"))) return s;
+  if ((s = Bt.upload(&Bt.d_exps, hexps, "upload batch exponents"))) return s;
+  if ((s = Bt.upload(&Bt.d_coefs, hcoefs, "upload batch coefficients"))) return s;
+  if ((s = Bt.upload(&Bt.d_work, work, "upload batch work list"))) return s;
+  if ((s = Bt.alloc((void**)&Bt.d_prims, (size_t)std::max<long long>(pp0, 1) * sizeof(PrimPair),
+                    "cudaMalloc(batch primitive pairs)")))
+    return s;
+  const int np = (int)pairs.size();
+  pair_precompute<<<(np + 127) / 128, 128>>>(Bt.d_pairs, np, Bt.d_shells, Bt.d_exps, Bt.d_coefs,
+                                             Bt.d_prims);
+  GBX_CUDA(cudaGetLastError(), "pair_precompute launch");
+  if ((s = boys_table(Bt.device, &Bt.d_boys))) return s;
+  for (size_t k = 0; k < Bt.types.size(); ++k) {
+    if ((s = Bt.upload(&Bt.types[k].d_base, tbase[k], "upload batch block bases"))) return s;
+    if ((s = Bt.upload(&Bt.types[k].d_ncols, tcols[k], "upload batch block columns"))) return s;
+  }
+  if ((s = Bt.alloc((void**)&Bt.d_compact, (size_t)Bt.compact_elems * sizeof(double),
+                    "cudaMalloc(batch compact store)")))
+    return s;
+
+  // expansion tables and descriptors
+  std::vector<int> gtab;
+  std::vector<int4> rowinfo;
+  std::vector<BlockDev> blocks;
+  std::vector<long long> goff, roff, boff;
+  std::vector<long long> row_first(n_mol + 1, 0);
+  for (int m = 0; m < n_mol; ++m) {
+    const Basis& B = *Bt.mols[m];
+    goff.push_back((long long)gtab.size());
+    roff.push_back((long long)rowinfo.size());
+    boff.push_back((long long)blocks.size());
+    gtab.insert(gtab.end(), B.h_gtab.begin(), B.h_gtab.end());
+    rowinfo.insert(rowinfo.end(), B.h_rowinfo.begin(), B.h_rowinfo.end());
+    blocks.insert(blocks.end(), B.block_table.begin(), B.block_table.end());
+    const long long npf = B.pf_first[kNumPairClasses];
+    row_first[m + 1] = row_first[m] + npf;
+    Bt.max_row_bytes = std::max(Bt.max_row_bytes, (size_t)npf * sizeof(double));
+  }
+  Bt.total_rows = row_first[n_mol];
+  if ((s = Bt.upload(&Bt.d_gtab, gtab, "upload batch gtab"))) return s;
+  if ((s = Bt.upload(&Bt.d_rowinfo, rowinfo, "upload batch rowinfo"))) return s;
+  if ((s = Bt.upload(&Bt.d_blocks, blocks, "upload batch block tables"))) return s;
+  if ((s = Bt.upload(&Bt.d_row_first, row_first, "upload batch row offsets"))) return s;
+  Bt.h_exp.resize(n_mol);
+  for (int m = 0; m < n_mol; ++m) {
+    const Basis& B = *Bt.mols[m];
+    ExpandArgs e;
+    memset(&e, 0, sizeof(e));
+    e.n = B.nbf;
+    e.nsh = (int)B.shells.size();
+    e.notation = GBX_CHEMIST;
+    e.blocks = Bt.d_blocks + boff[m];
+    e.compact = Bt.d_compact + Bt.compact_off[m];
+    e.out = nullptr;
+    e.gtab = Bt.d_gtab + goff[m];
+    e.rowinfo = Bt.d_rowinfo + roff[m];
+    e.npf = B.pf_first[kNumPairClasses];
+    for (int c = 0; c <= kNumPairClasses; ++c) e.pf_first[c] = B.pf_first[c];
+    Bt.h_exp[m] = e;
+  }
+  if ((s = Bt.alloc((void**)&Bt.d_exp, n_mol * sizeof(ExpandArgs), "cudaMalloc(batch descriptors)")))
+    return s;
+  GBX_CUDA(cudaStreamCreateWithFlags(&Bt.exec, cudaStreamNonBlocking), "create stream");
+  Bt.aux.resize(kAuxStreams);
+  Bt.join.resize(kAuxStreams);
+  for (int j = 0; j < kAuxStreams; ++j) {
+    GBX_CUDA(cudaStreamCreateWithFlags(&Bt.aux[j], cudaStreamNonBlocking), "create stream");
+    GBX_CUDA(cudaEventCreateWithFlags(&Bt.join[j], cudaEventDisableTiming), "create event");
+  }
+  GBX_CUDA(cudaEventCreateWithFlags(&Bt.fork, cudaEventDisableTiming), "create event");
+  GBX_CUDA(cudaEventCreateWithFlags(&Bt.ev_in, cudaEventDisableTiming), "create event");
+  GBX_CUDA(cudaEventCreateWithFlags(&Bt.ev_out, cudaEventDisableTiming), "create event");
+  GBX_CUDA(cudaDeviceSynchronize(), "batch upload");
+  return GBX_OK;
+}
+
+// The launches of one batch run on stream `st` (class kernels on the auxiliary streams).
+static int enqueue_batch(Batch& Bt, cudaStream_t st) {
+  const int nsm = num_sms_of(Bt.device);
+  GBX_CUDA(cudaEventRecord(Bt.fork, st), "fork");
+  for (cudaStream_t a : Bt.aux) GBX_CUDA(cudaStreamWaitEvent(a, Bt.fork, 0), "fork wait");
+  for (size_t i = 0; i < Bt.order.size(); ++i) {
+    const BatchType& T = Bt.types[Bt.order[i]];
+    EriLaunch a;
+    memset(&a, 0, sizeof(a));
+    a.pairs = Bt.d_pairs;
+    a.prims = Bt.d_prims;
+    a.shells = Bt.d_shells;
+    a.boys_tab = Bt.d_boys;
+    a.out = Bt.d_compact;
+    a.work = Bt.d_work;
+    a.work_off = T.work_off;
+    a.nwork = T.n;
+    a.mode = 0;
+    a.team = T.team;
+    a.mol_base = T.d_base;
+    a.mol_ncols = T.d_ncols;
+    const int grid = (int)std::max<long long>(
+        1, std::min<long long>((T.n * T.team + 127) / 128, (long long)nsm * 8));
+    int s = launch_class(kPairClassL[T.cb][0], kPairClassL[T.cb][1], kPairClassL[T.ck][0],
+                         kPairClassL[T.ck][1], a, grid, Bt.aux[i % Bt.aux.size()]);
+    if (s) return s;
+  }
+  for (size_t j = 0; j < Bt.aux.size(); ++j) {
+    GBX_CUDA(cudaEventRecord(Bt.join[j], Bt.aux[j]), "join");
+    GBX_CUDA(cudaStreamWaitEvent(st, Bt.join[j], 0), "join wait");
+  }
+  return launch_expand_batch(Bt.device, Bt.d_exp, Bt.d_row_first, Bt.nmol, Bt.total_rows,
+                             Bt.max_row_bytes, st);
+}
+
+static int run_batch(Batch& Bt, int notation, double* const* outs, cudaStream_t caller) {
+  for (int m = 0; m < Bt.nmol; ++m)
+    if (!outs[m]) return set_error(GBX_ERR_INVALID, "output of molecule %d is null", m);
+  bool changed = Bt.exp_dirty;
+  for (int m = 0; m < Bt.nmol; ++m) {
+    if (Bt.h_exp[m].out != outs[m] || Bt.h_exp[m].notation != notation) changed = true;
+    Bt.h_exp[m].out = outs[m];
+    Bt.h_exp[m].notation = notation;
+  }
+  GBX_CUDA(cudaEventRecord(Bt.ev_in, caller), "record caller");
+  GBX_CUDA(cudaStreamWaitEvent(Bt.exec, Bt.ev_in, 0), "wait caller");
+  if (changed) {
+    Bt.exp_dirty = true;  // until the device table holds these outputs
+    GBX_CUDA(cudaMemcpyAsync(Bt.d_exp, Bt.h_exp.data(), Bt.nmol * sizeof(ExpandArgs),
+                             cudaMemcpyHostToDevice, Bt.exec), "upload batch descriptors");
+    GBX_CUDA(cudaStreamSynchronize(Bt.exec), "upload batch descriptors");
+    Bt.exp_dirty = false;
+  }
+  if (Bt.use_graph && !Bt.graph_exec) {
+    GBX_CUDA(cudaStreamBeginCapture(Bt.exec, cudaStreamCaptureModeRelaxed), "begin capture");
+    const int s = enqueue_batch(Bt, Bt.exec);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(Bt.exec, &g);
+    if (s) {
+      if (g) cudaGraphDestroy(g);
+      return s;
+    }
+    GBX_CUDA(e, "end capture");
+    Bt.graph = g;
+    GBX_CUDA(cudaGraphInstantiate(&Bt.graph_exec, g, 0), "instantiate batch graph");
+  }
+  if (Bt.use_graph) {
+    GBX_CUDA(cudaGraphLaunch(Bt.graph_exec, Bt.exec), "launch batch graph");
+  } else {
+    const int s = enqueue_batch(Bt, Bt.exec);
+    if (s) return s;
+  }
+  GBX_CUDA(cudaEventRecord(Bt.ev_out, Bt.exec), "record batch");
+  GBX_CUDA(cudaStreamWaitEvent(caller, Bt.ev_out, 0), "caller wait");
+  return GBX_OK;
+}
+
+}  // namespace gbx
+
+using namespace gbx;
+
+struct gbx_batch {
+  std::unique_ptr<Batch> impl;
+};
+
+int gbx_batch_create(gbx_batch** out, int n_mol, const int* mol_nshells, const int* angmom,
+                     const int* nprim, const double* center, const double* exps,
+                     const double* coefs, const int* nout, const int* sph, const int8_t* pos,
+                     const double* scl, int device) {
+  if (!out || n_mol <= 0 || !mol_nshells || !angmom || !nprim || !center || !exps || !coefs ||
+      !nout || !sph || !pos || !scl)
+    return set_error(GBX_ERR_INVALID, "gbx_batch_create: null argument or empty batch");
+  *out = nullptr;
+  int ndev = 0;
+  GBX_CUDA(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+  if (device < 0 || device >= ndev)
+    return set_error(GBX_ERR_INVALID, "device %d not present (%d devices)", device, ndev);
+  auto B = std::make_unique<Batch>();
+  B->device = device;
+  DeviceGuardLite g(device);
+  const int s = build_batch(*B, n_mol, mol_nshells, angmom, nprim, center, exps, coefs, nout,
+                            sph, pos, scl);
+  if (s) return s;
+  *out = new gbx_batch{std::move(B)};
+  return GBX_OK;
+}
+
+int gbx_batch_destroy(gbx_batch* b) {
+  delete b;
+  return GBX_OK;
+}
+
+int gbx_batch_info(const gbx_batch* b, int64_t* nbf, int64_t* n_quartets, int64_t* compact_bytes) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_batch_info: null batch");
+  const Batch& B = *b->impl;
+  if (nbf)
+    for (int m = 0; m < B.nmol; ++m) nbf[m] = B.mols[m]->nbf;
+  if (n_quartets) *n_quartets = B.n_quartets;
+  if (compact_bytes) *compact_bytes = B.compact_elems * (int64_t)sizeof(double);
+  return GBX_OK;
+}
+
+int gbx_batch_set_graph(gbx_batch* b, int on) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_batch_set_graph: null batch");
+  b->impl->use_graph = on != 0;
+  return GBX_OK;
+}
+
+int gbx_batch_run(gbx_batch* b, int notation, double* const* outs, void* stream) {
+  if (!b || !outs) return set_error(GBX_ERR_INVALID, "gbx_batch_run: null argument");
+  if (notation != GBX_CHEMIST && notation != GBX_PHYSICIST)
+    return set_error(GBX_ERR_INVALID, "notation must be GBX_CHEMIST or GBX_PHYSICIST");
+  Batch& B = *b->impl;
+  DeviceGuardLite g(B.device);
+  return run_batch(B, notation, outs, (cudaStream_t)stream);
+}

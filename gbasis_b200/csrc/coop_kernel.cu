@@ -275,7 +275,9 @@ __global__ void eri_coop(const CoopArgs A) {
     // ---------------------------------------------------------------- D
     const int ncol = nCi * nDi;
     const long long nBo = sB.nout, nDo = sD.nout;
-    double* __restrict__ dst = a.out + a.base + Q.fo;
+    long long bbase, bcols;
+    block_dest(a, P, bbase, bcols);
+    double* __restrict__ dst = a.out + bbase + Q.fo;
     for (int c0 = 0; c0 < ncol; c0 += A.Cc) {
       const int cc = min(A.Cc, ncol - c0);
       for (int i = lane; i < cc * M.NE; i += 32) {
@@ -361,7 +363,7 @@ __global__ void eri_coop(const CoopArgs A) {
         }
         const double v = OB[c * NAB + ua * nBi + ub] * sA.scl[ua] * sB.scl[ub] * sC.scl[uc] *
                          sD.scl[ud];
-        dst[((long long)P.fo + sA.pos[ua] * nBo + sB.pos[ub]) * a.ncols + sC.pos[uc] * nDo +
+        dst[((long long)P.fo + sA.pos[ua] * nBo + sB.pos[ub]) * bcols + sC.pos[uc] * nDo +
             sD.pos[ud]] = v;
       }
       __syncwarp();

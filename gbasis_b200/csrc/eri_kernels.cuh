@@ -285,7 +285,9 @@ __global__ void __launch_bounds__(kEriThreads) eri_block(const EriLaunch a) {
       continue;
     }
     const long long nBo = sB.nout, nDo = sD.nout;
-    double* __restrict__ dst = a.out + a.base + Q.fo;
+    long long bbase, bcols;
+    block_dest(a, P, bbase, bcols);
+    double* __restrict__ dst = a.out + bbase + Q.fo;
 #pragma unroll
     for (int ia = 0; ia < NCA; ++ia) {
       if (ia >= nAi) break;
@@ -295,7 +297,7 @@ __global__ void __launch_bounds__(kEriThreads) eri_block(const EriLaunch a) {
       for (int ib = 0; ib < NCB; ++ib) {
         if (ib >= nBi) break;
         const double fab = fa * sB.scl[ib];
-        double* __restrict__ row = dst + (ra + sB.pos[ib]) * a.ncols;
+        double* __restrict__ row = dst + (ra + sB.pos[ib]) * bcols;
 #pragma unroll
         for (int ic = 0; ic < NCC; ++ic) {
           if (ic >= nCi) break;

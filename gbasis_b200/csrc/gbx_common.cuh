@@ -58,7 +58,8 @@ struct __align__(16) PrimPair {
 struct PairDev {
   int shA, shB, prim_off, nprim;
   int cls, local, fo, nB;  // class, index within class, pair-function offset in class, nout(B)
-  double ABx, ABy, ABz, pad;
+  double ABx, ABy, ABz;
+  int mol, pad;            // molecule of the pair in a batch (0 for a single basis)
 };
 
 // Per class block: where its quartets live in the work list and in the compact store.
@@ -89,6 +90,22 @@ struct EriLaunch {
   long long nbf;
   double* qout;             // per-pair Schwarz value (mode 1)
   int* status;              // device error flag
+  // batch of molecules: the block's base and column count in each molecule's compact store,
+  // indexed by PairDev::mol (nullptr: base / ncols above)
+  const long long* mol_base;
+  const long long* mol_ncols;
 };
+
+// Destination block of a quartet whose bra pair is P.
+__device__ __forceinline__ void block_dest(const EriLaunch& a, const PairDev& P, long long& base,
+                                           long long& ncols) {
+  if (a.mol_base) {
+    base = a.mol_base[P.mol];
+    ncols = a.mol_ncols[P.mol];
+  } else {
+    base = a.base;
+    ncols = a.ncols;
+  }
+}
 
 }  // namespace gbx

@@ -276,6 +276,34 @@ __global__ void __launch_bounds__(512) expand_rows(const ExpandArgs e) {
   }
 }
 
+// Batch form of the row-staged expansion: molecule m's pair-function rows are the global rows
+// [row_first[m], row_first[m + 1]); each molecule has its own descriptor (tables, compact
+// store, output).
+__global__ void __launch_bounds__(512) expand_rows_batch(const ExpandArgs* __restrict__ mols,
+                                                         const long long* __restrict__ row_first,
+                                                         int nmol) {
+  extern __shared__ double s_row[];
+  const long long total = row_first[nmol];
+  for (long long g = blockIdx.x; g < total; g += gridDim.x) {
+    int lo = 0, hi = nmol - 1;  // last molecule whose first row is <= g
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(row_first + mid) <= g) lo = mid;
+      else hi = mid - 1;
+    }
+    const ExpandArgs& e = mols[lo];
+    const bool phys = e.notation == GBX_PHYSICIST;
+    const long long r = g - row_first[lo];
+    const int4 ri = __ldg(e.rowinfo + r);
+    if (ri.x < 0) continue;
+    __syncthreads();
+    stage_row(e, r, ri.w, s_row);
+    __syncthreads();
+    write_plane(e, s_row, plane_ptr(e, e.out, ri.x, ri.y, phys), phys);
+    if (ri.z) write_plane(e, s_row, plane_ptr(e, e.out, ri.y, ri.x, phys), phys);
+  }
+}
+
 // Slab form of the row-staged expansion: the planes of x in [x0, x1) only — the contiguous
 // range out[x0 * N^3, x1 * N^3) — into dst (which holds that range), one plane per ordered
 // pair (x, y).  Used to stream the tensor to host memory slab by slab.
@@ -651,10 +679,10 @@ static ExpandArgs expand_args(const Basis& B, int notation, double* out) {
 // CTAs per SM of a row-staged expansion kernel with one M row in shared memory (0 when the
 // row does not fit).
 template <typename K>
-static int row_kernel_fit(const Basis& B, K kernel, size_t row_bytes, int* per_sm) {
+static int row_kernel_fit(int device, K kernel, size_t row_bytes, int* per_sm) {
   *per_sm = 0;
   int optin = 0;
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, B.device);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   if (row_bytes > (size_t)optin) return GBX_OK;
   if (row_bytes > 48 * 1024)
     GBX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -663,6 +691,26 @@ static int row_kernel_fit(const Basis& B, K kernel, size_t row_bytes, int* per_s
            "expansion occupancy");
   return GBX_OK;
 }
+
+// Row-staged expansion of a batch of molecules (descriptors and row offsets on the device).
+int launch_expand_batch(int device, const ExpandArgs* d_mols, const long long* d_row_first,
+                        int nmol, long long total_rows, size_t max_row_bytes, cudaStream_t st) {
+  int per_sm = 0, s;
+  if ((s = row_kernel_fit(device, expand_rows_batch, max_row_bytes, &per_sm))) return s;
+  if (per_sm == 0)
+    return set_error(GBX_ERR_UNSUPPORTED, "a molecule's pair-function row (%zu bytes) exceeds "
+                     "shared memory", max_row_bytes);
+  const int grid = (int)std::max<long long>(
+      1, std::min<long long>(total_rows, (long long)num_sms(device) * per_sm));
+  expand_rows_batch<<<grid, 512, max_row_bytes, st>>>(d_mols, d_row_first, nmol);
+  return cuda_status(cudaGetLastError(), "expand_rows_batch launch");
+}
+
+ExpandArgs make_expand_args(const Basis& B, int notation, double* out) {
+  return expand_args(B, notation, out);
+}
+
+int num_sms_of(int device) { return num_sms(device); }
 
 // Full tensor into host memory without an N^4 device buffer: after the class kernels, the
 // tensor is expanded slab by slab (x-ranges of out[x, ...], each a contiguous host range)
@@ -674,7 +722,7 @@ int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStre
   const size_t slab = (size_t)n * n * n;  // elements of one x
   const size_t row_bytes = (size_t)B.pf_first[kNumPairClasses] * sizeof(double);
   int per_sm = 0, s;
-  if ((s = row_kernel_fit(B, expand_slab, row_bytes, &per_sm))) return s;
+  if ((s = row_kernel_fit(B.device, expand_slab, row_bytes, &per_sm))) return s;
   if (per_sm == 0) {
     // a pair-function row larger than shared memory: whole tensor on the device, one copy
     if ((s = B.ensure_out((size_t)n * slab))) return s;
@@ -739,7 +787,7 @@ int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, d
   if (B.profiling) cudaEventRecord(B.ev[2], st);
   const size_t row_bytes = (size_t)e.npf * sizeof(double);
   int per_sm = 0;
-  if ((s = row_kernel_fit(B, expand_rows, row_bytes, &per_sm))) return s;
+  if ((s = row_kernel_fit(B.device, expand_rows, row_bytes, &per_sm))) return s;
   if (per_sm > 0) {
     // one pair-function row of M in shared memory per CTA; persistent grid of the CTAs that
     // fit on the SMs together

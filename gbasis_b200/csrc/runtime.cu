@@ -30,6 +30,8 @@ int set_error(int code, const char* fmt, ...) {
   return code;
 }
 
+const char* gbx_last_error_str() { return g_last_error.c_str(); }
+
 int cuda_status(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return GBX_OK;
   if (e == cudaErrorMemoryAllocation)

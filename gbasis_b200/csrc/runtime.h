@@ -115,6 +115,11 @@ int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStre
 int run_compact(Basis& B, double tau, cudaStream_t st, double skip = 0.0, double fp32 = 0.0);
 int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st);
 int ensure_schwarz(Basis& B, cudaStream_t st);
+struct ExpandArgs;
+int launch_expand_batch(int device, const ExpandArgs* d_mols, const long long* d_row_first,
+                        int nmol, long long total_rows, size_t max_row_bytes, cudaStream_t st);
+ExpandArgs make_expand_args(const Basis& B, int notation, double* out);
+int num_sms_of(int device);
 int launch_class(int la, int lb, int lc, int ld, const EriLaunch& a, int grid, cudaStream_t st);
 
 }  // namespace gbx

@@ -130,6 +130,29 @@ int gbx_eri_full_noalloc(int n_shells, const int* angmom, const int* nprim,
                          const int* nout, const int* sph, const int8_t* pos, const double* scl,
                          int notation, double* out, void* stream);
 
+/*
+ * Batched full tensors of many molecules (no counterpart in the reference: gbasis computes
+ * one basis per electron_repulsion_integral call; this replaces a Python loop of such calls).
+ * The molecules' shells are given back to back in the gbx_basis_create arrays, molecule m
+ * owning mol_nshells[m] consecutive shells.  gbx_batch_run writes molecule m's N_m^4 float64
+ * tensor to the device buffer outs[m] (host array of n_mol device pointers); the first run
+ * captures all launches — one class kernel per block type for the whole batch, then one
+ * batched expansion — into a CUDA graph that later runs replay (with any outputs and
+ * notation).  Ordered after prior work on `stream` and before later work on it.
+ */
+typedef struct gbx_batch gbx_batch;
+int gbx_batch_create(gbx_batch** out, int n_mol, const int* mol_nshells, const int* angmom,
+                     const int* nprim, const double* center, const double* exps,
+                     const double* coefs, const int* nout, const int* sph, const int8_t* pos,
+                     const double* scl, int device);
+int gbx_batch_destroy(gbx_batch* b);
+/* nbf: n_mol entries (may be NULL); total unique shell quartets; compact store bytes. */
+int gbx_batch_info(const gbx_batch* b, int64_t* nbf, int64_t* n_quartets,
+                   int64_t* compact_bytes);
+int gbx_batch_run(gbx_batch* b, int notation, double* const* outs, void* stream);
+/* 1 (default): replay a captured CUDA graph; 0: launch eagerly every run. */
+int gbx_batch_set_graph(gbx_batch* b, int on);
+
 /* Coulomb matrix J[a,b] = sum_cd (ab|cd) D[c,d] from the screened unique quartets
  * (full tensor never stored).  D, J: device N x N row-major (D symmetric). */
 int gbx_eri_coulomb_j(gbx_basis* b, const double* D, double schwarz_threshold, double* J,

@@ -1,0 +1,89 @@
+"""GPU tests of the batched form (one CUDA graph for many molecules) through the C ABI.
+
+Each molecule's tensor must match the single-molecule path (same kernels; the team of lanes
+sharing a quartet may differ, which changes only the order of the primitive sums) and, for
+small molecules, the oracle at the FP64 bar of 1e-12.
+"""
+import numpy as np
+import pytest
+
+from gbasis_b200 import _engine
+from gbasis_b200.batch import EriBatch, electron_repulsion_integral_batch
+from gbasis_b200.synthetic import batch_molecule, make_workload
+from oracle import eri_oracle as orc
+
+pytestmark = pytest.mark.gpu
+ATOL = 1e-12
+
+
+def _single(shells, notation="chemist"):
+    import torch
+    db = _engine.DeviceBasis(shells)
+    n = db.nbf
+    out = torch.empty(n ** 4, dtype=torch.float64, device="cuda")
+    db.full_device(out.data_ptr(), notation)
+    torch.cuda.synchronize()
+    db.close()
+    return out.cpu().numpy().reshape((n,) * 4)
+
+
+def test_batch_matches_single_molecule_path_and_replays():
+    import torch
+    mols = [batch_molecule(m) for m in range(24)]
+    b = EriBatch(mols)
+    assert b.n_mol == 24
+    outs = [torch.full((n,) * 4, np.nan, dtype=torch.float64, device="cuda") for n in b.nbf]
+    b.run(outs)  # captures the graph
+    torch.cuda.synchronize()
+    for m in range(0, 24, 3):
+        np.testing.assert_allclose(outs[m].cpu().numpy(), _single(mols[m]), rtol=0, atol=1e-13)
+    # replay into fresh buffers, physicist notation
+    outs2 = [torch.full((n,) * 4, np.nan, dtype=torch.float64, device="cuda") for n in b.nbf]
+    b.run(outs2, "physicist")
+    torch.cuda.synchronize()
+    for m in range(24):
+        np.testing.assert_array_equal(outs2[m].cpu().numpy(),
+                                      outs[m].permute(0, 2, 1, 3).contiguous().cpu().numpy())
+    b.close()
+
+
+def test_batch_eager_equals_graph():
+    import torch
+    mols = [batch_molecule(m) for m in range(40, 52)]
+    g = EriBatch(mols)
+    e = EriBatch(mols, graph=False)
+    og = [torch.empty((n,) * 4, dtype=torch.float64, device="cuda") for n in g.nbf]
+    oe = [torch.empty((n,) * 4, dtype=torch.float64, device="cuda") for n in e.nbf]
+    g.run(og)
+    e.run(oe)
+    torch.cuda.synchronize()
+    for a, b in zip(og, oe):
+        assert torch.equal(a, b)
+    g.close()
+    e.close()
+
+
+def test_batch_small_molecules_against_oracle():
+    mols = [make_workload("tiny4")] + [m for m in (batch_molecule(k) for k in range(200))
+                                       if sum(len(s.angmom_components_cart) for s in m) <= 24][:3]
+    got = electron_repulsion_integral_batch(mols, notation="chemist")
+    for shells, t in zip(mols, got):
+        ref = orc.electron_repulsion_integral(shells, notation="chemist", reorder="exponent")
+        np.testing.assert_allclose(t.cpu().numpy(), ref, rtol=0, atol=ATOL)
+
+
+def test_batch_rejects_bad_outputs():
+    import torch
+    mols = [batch_molecule(m) for m in range(3)]
+    b = EriBatch(mols)
+    outs = [torch.empty((n,) * 4, dtype=torch.float64, device="cuda") for n in b.nbf]
+    with pytest.raises(ValueError):
+        b.run(outs[:2])
+    wrong = torch.empty(b.nbf[0] ** 4 + 1, dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError):
+        b.run([wrong] + outs[1:])
+    with pytest.raises(ValueError):  # null device pointer, rejected by the C ABI
+        b.run([0] + [o.data_ptr() for o in outs[1:]])
+    with pytest.raises(ValueError):
+        b.run(outs, "neither")
+    b.close()
