@@ -194,6 +194,105 @@ def run_reference(a, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def extra_configs(local, reps=2):
+    """The other configurations of the path, each timed on the device with CUDA events on the
+    launching stream (one warm-up call, then ``reps`` calls):
+
+    * ``chain20_unique``: 20-atom random-walk chain, 140 spherical shells (s,s,s,p,p,d,f per
+      atom), N = 420; the 8-fold unique integrals only (no N^4 tensor), FP64 and mixed form,
+      with the mixed form's max error over the whole compact store;
+    * ``batch512``: 512 molecules of 2-14 atoms, one CUDA graph per run (every molecule's full
+      Cartesian tensor, device resident);
+    * ``large64_coulomb_subset``: direct Coulomb matrix of the first 16 atoms of the 64-atom
+      box (160 spherical shells, N = 480; the full 64-atom system takes minutes).
+    """
+    import ctypes
+    import torch
+    from gbasis_b200 import _engine
+    from gbasis_b200.batch import EriBatch
+    from gbasis_b200.electron_repulsion import MIXED_FP32, MIXED_SKIP
+    from gbasis_b200.flops import basis_flops, unique_eris
+    from gbasis_b200.synthetic import density_matrix, make_workload
+    dev = torch.device("cuda", local)
+    st = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(st.cuda_stream)
+    peak64 = _engine.fp64_peak(local)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+    shells = make_workload("chain20")
+    db = _engine.DeviceBasis(shells, device=local)
+    uq, fl = unique_eris(db.nbf), basis_flops(shells)
+    ms64 = timed(lambda: db.unique(stream=sp))
+    ref = db.compact_view().clone()
+    msmx = timed(lambda: db.unique((MIXED_SKIP, MIXED_FP32), stream=sp))
+    cur = db.compact_view()
+    max_abs = max_rel = 0.0
+    for c0 in range(0, ref.numel(), 1 << 27):
+        r, x = ref[c0:c0 + (1 << 27)], cur[c0:c0 + (1 << 27)]
+        d = (x - r).abs()
+        max_abs = max(max_abs, float(d.max()))
+        max_rel = max(max_rel, float((d / r.abs().clamp_min(1e-8)).max()))
+    out["chain20_unique"] = {
+        "n_functions": db.nbf, "unique_eris": uq, "shell_quartets": db.stats()[0],
+        "fp64": {"ms": ms64, "value": uq / (ms64 * 1e-3), "unit": UNIT,
+                 "achieved_tflops": fl / (ms64 * 1e-3) / 1e12, "frac_fp64_peak": fl / (ms64 * 1e-3) / 1e12 / peak64},
+        "mixed": {"ms": msmx, "value": uq / (msmx * 1e-3), "unit": UNIT, "speedup_vs_fp64": ms64 / msmx,
+                  "max_abs_err_vs_fp64": max_abs, "max_rel_err_vs_fp64": max_rel,
+                  "error_over": "every unique integral", "skip_bound": MIXED_SKIP,
+                  "fp32_bound": MIXED_FP32}}
+    del ref, cur, r, x, d
+    db.close()
+    torch.cuda.empty_cache()
+
+    mols = make_workload("batch512")
+    t0 = time.perf_counter()
+    b = EriBatch(mols, device=local)
+    t_create = time.perf_counter() - t0
+    outs = [torch.empty((n,) * 4, dtype=torch.float64, device=dev) for n in b.nbf]
+    ms = timed(lambda: b.run(outs, stream=sp))
+    uq = sum(unique_eris(n) for n in b.nbf)
+    fl = sum(basis_flops(m) for m in mols)
+    out["batch512"] = {
+        "molecules": len(mols), "unique_eris": uq, "shell_quartets": b.n_quartets,
+        "tensor_bytes": 8 * sum(n ** 4 for n in b.nbf), "ms": ms,
+        "value": uq / (ms * 1e-3), "unit": UNIT, "molecules_per_s": len(mols) / (ms * 1e-3),
+        "achieved_tflops": fl / (ms * 1e-3) / 1e12, "frac_fp64_peak": fl / (ms * 1e-3) / 1e12 / peak64,
+        "create_s": t_create, "launch": "one CUDA graph replay per run"}
+    b.close()
+    del outs
+    torch.cuda.empty_cache()
+
+    shells = make_workload("large64")[:160]
+    db = _engine.DeviceBasis(shells, device=local)
+    n = db.nbf
+    D = torch.from_numpy(density_matrix(n)).to(dev)
+    J = torch.empty((n, n), dtype=torch.float64, device=dev)
+
+    def coulomb():
+        _engine.check(_engine.lib().gbx_eri_coulomb_j(
+            db.handle, ctypes.c_void_p(D.data_ptr()), 1e-12, ctypes.c_void_p(J.data_ptr()), sp),
+            "gbx_eri_coulomb_j")
+    ms = timed(coulomb)
+    nq = db.stats()[0]
+    out["large64_coulomb_subset"] = {
+        "atoms": 16, "n_functions": n, "shell_quartets": nq, "schwarz_threshold": 1e-12,
+        "ms": ms, "quartets_per_s": nq / (ms * 1e-3), "unit": "shell quartets/s (before screening)"}
+    db.close()
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -202,6 +301,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-extra-configs", action="store_true",
+                    help="skip the chain20 / batch512 / large64-subset measurements")
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -332,8 +433,12 @@ def main():
             "e2e": e2e, "clocks": clk.summary(), "mixed": mixed,
             "gpu_launches": None}
     # our kernels per step: work-list build + one per class block + expansion
-    import gbasis_b200._engine as eng  # noqa: F401
-    line["gpu_launches"] = a.steps * (2 + _num_blocks(shells))
+    line["gpu_launches"] = a.steps * (2 + len(db.blocks()))
+    db.close()
+    if world == 1 and not a.no_extra_configs:
+        del out
+        torch.cuda.empty_cache()
+        line["configs"] = extra_configs(local)
     if rank == 0 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(shells)
     if rank == 0:
@@ -342,14 +447,6 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-
-
-def _num_blocks(shells):
-    ls = set()
-    for s in shells:
-        ls.add(s.angmom)
-    pcs = sorted({(max(a, b), min(a, b)) for a in ls for b in ls})
-    return len(pcs) * (len(pcs) + 1) // 2
 
 
 if __name__ == "__main__":

@@ -30,7 +30,7 @@ EXPORTED_SYMBOLS = (
     "gbx_num_blocks", "gbx_block_info", "gbx_set_team", "gbx_block_times",
     "gbx_eri_full_mixed", "gbx_eri_unique",
     "gbx_batch_create", "gbx_batch_destroy", "gbx_batch_info", "gbx_batch_run",
-    "gbx_batch_set_graph",
+    "gbx_batch_set_graph", "gbx_unique_values", "gbx_compact_view",
 )
 
 
@@ -91,6 +91,8 @@ def lib():
             "gbx_batch_info": [_P, _P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
             "gbx_batch_run": [_P, _I, _P, _P],
             "gbx_batch_set_graph": [_P, _I],
+            "gbx_unique_values": [_P, _I64, _P, _P, _P],
+            "gbx_compact_view": [_P, ctypes.POINTER(_P), ctypes.POINTER(_I64)],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -284,6 +286,28 @@ class DeviceBasis:
         """Unique quartets into the engine's compact store (no expansion)."""
         check(lib().gbx_eri_unique(self.handle, float(mixed[0]), float(mixed[1]), stream),
               "gbx_eri_unique")
+
+    def unique_values(self, idx4, stream=None):
+        """(ab|cd) for rows (a, b, c, d) of ``idx4`` from the last call's compact store."""
+        q = np.ascontiguousarray(np.asarray(idx4, dtype=np.int64).reshape(-1, 4))
+        out = np.empty(len(q))
+        check(lib().gbx_unique_values(self.handle, len(q), _ptr(q), _ptr(out), stream),
+              "gbx_unique_values")
+        return out
+
+    def compact_view(self):
+        """The compact store of the last call as a read-only 1-D float64 CUDA tensor (a view
+        of engine memory, valid until the next call on this basis), or None."""
+        import torch
+        p, n = ctypes.c_void_p(), ctypes.c_int64()
+        check(lib().gbx_compact_view(self.handle, ctypes.byref(p), ctypes.byref(n)))
+        if not p.value or n.value == 0:
+            return None
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (int(n.value),), "typestr": "<f8",
+                                        "data": (int(p.value), False), "version": 3}
+        return torch.as_tensor(_View(), device=torch.device("cuda", self.device))
 
     def schwarz_bounds(self):
         ns = len(self.packed["angmom"])

@@ -6,13 +6,18 @@
 //   K6 expand_full       — the 8-fold symmetric N^4 tensor from the compact store,
 //                          coalesced writes in chemist or physicist order
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <memory>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "gbx_eri.h"
 #include "gbx_common.cuh"
 #include "pipeline_kernels.cuh"
+#include "coop.cuh"
 #include "runtime.h"
 
 namespace gbx {
@@ -121,7 +126,7 @@ __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* _
       // of each shell) decides skip (< skip), FP32 (< fp32) or FP64
       const double bnd = mp.qm[p] * mp.qm[q];
       if (bnd < mp.skip) pass = false;
-      fp32 = pass && bnd < mp.fp32;
+      fp32 = pass && B.fp32_ok && bnd < mp.fp32;
     }
   }
   const bool p64 = pass && !fp32;
@@ -220,14 +225,25 @@ __device__ __forceinline__ void stage_row(const ExpandArgs& e, long long r, int 
   for (int Y = 0; Y < kNumPairClasses; ++Y) {
     const long long y0 = e.pf_first[Y], ny = e.pf_first[Y + 1] - y0;
     if (ny == 0) continue;
-    if (X > Y) {
-      const BlockDev b = e.blocks[X * kNumPairClasses + Y];
-      const double* __restrict__ src = e.compact + b.base + rho * b.ncols;
-      for (long long j = tid; j < ny; j += nt) s_row[y0 + j] = __ldg(src + j);
-    } else if (X < Y) {
-      const BlockDev b = e.blocks[Y * kNumPairClasses + X];
-      const double* __restrict__ src = e.compact + b.base + rho;
-      for (long long j = tid; j < ny; j += nt) s_row[y0 + j] = __ldg(src + j * b.ncols);
+    if (X != Y) {
+      // a row of block (X, Y) (unit stride) or a column of block (Y, X) (stride = columns);
+      // four loads in flight per thread
+      const BlockDev b = X > Y ? e.blocks[X * kNumPairClasses + Y] : e.blocks[Y * kNumPairClasses + X];
+      const double* __restrict__ src = e.compact + b.base + (X > Y ? rho * b.ncols : rho);
+      const long long stride = X > Y ? 1 : b.ncols;
+      for (long long j0 = tid; j0 < ny; j0 += 4LL * nt) {
+        double v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const long long j = j0 + (long long)k * nt;
+          v[k] = j < ny ? __ldg(src + j * stride) : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const long long j = j0 + (long long)k * nt;
+          if (j < ny) s_row[y0 + j] = v[k];
+        }
+      }
     } else {
       const BlockDev b = e.blocks[X * kNumPairClasses + X];
       const double* __restrict__ blk = e.compact + b.base;
@@ -245,13 +261,28 @@ __device__ __forceinline__ void write_plane(const ExpandArgs& e, const double* _
                                             double* __restrict__ dst, bool phys) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const long long n = e.n, n2 = n * n;
-  if (!phys) {
-    for (long long t = tid; t < n2; t += nt) __stcs(dst + t, s_row[__ldg(e.gtab + t)]);
-  } else {
-    const unsigned un = (unsigned)n;
-    for (unsigned t = tid; t < (unsigned)n2; t += nt) {
-      const unsigned c = t / un, d = t - c * un;
-      __stcs(dst + (long long)c * n2 + d, s_row[__ldg(e.gtab + t)]);
+  const int* __restrict__ gtab = e.gtab;
+  // four independent elements per thread per step (table loads in flight together); each
+  // of the four stores is coalesced across the warp
+  const unsigned un = (unsigned)n, un2 = (unsigned)n2;
+  for (unsigned t0 = tid; t0 < un2; t0 += 4u * nt) {
+    int g[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const unsigned t = t0 + k * nt;
+      g[k] = t < un2 ? __ldg(gtab + t) : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const unsigned t = t0 + k * nt;
+      if (t < un2) {
+        long long o = t;
+        if (phys) {
+          const unsigned c = t / un, d = t - c * un;
+          o = (long long)c * n2 + d;
+        }
+        __stcs(dst + o, s_row[g[k]]);
+      }
     }
   }
 }
@@ -274,6 +305,30 @@ __global__ void __launch_bounds__(512) expand_rows(const ExpandArgs e) {
     write_plane(e, s_row, plane_ptr(e, e.out, ri.x, ri.y, phys), phys);
     if (ri.z) write_plane(e, s_row, plane_ptr(e, e.out, ri.y, ri.x, phys), phys);
   }
+}
+
+// (ab|cd) of n function quadruples (a, b, c, d) from the compact store (indices checked by
+// the host to be below N).
+__global__ void gather_unique(const ExpandArgs e, const long long* __restrict__ idx4, long long n,
+                              double* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long a = idx4[4 * i], b = idx4[4 * i + 1], c = idx4[4 * i + 2], d = idx4[4 * i + 3];
+  const long long p = e.gtab[a * e.n + b], q = e.gtab[c * e.n + d];
+  int X = 0, Y = 0;
+  while (p >= e.pf_first[X + 1]) ++X;
+  while (q >= e.pf_first[Y + 1]) ++Y;
+  const long long rp = p - e.pf_first[X], rq = q - e.pf_first[Y];
+  const int lp = e.rowinfo[p].w, lq = e.rowinfo[q].w;
+  long long off;
+  if (X > Y || (X == Y && lp >= lq)) {
+    const BlockDev bd = e.blocks[X * kNumPairClasses + Y];
+    off = bd.base + rp * bd.ncols + rq;
+  } else {
+    const BlockDev bd = e.blocks[Y * kNumPairClasses + X];
+    off = bd.base + rq * bd.ncols + rp;
+  }
+  out[i] = e.compact[off];
 }
 
 // Batch form of the row-staged expansion: molecule m's pair-function rows are the global rows
@@ -406,6 +461,13 @@ int upload_basis(Basis& B) {
   return GBX_OK;
 }
 
+// Light classes run the register kernel, which has the FP32 path of the mixed form; the
+// cooperative kernel of the heavy classes computes every quartet in FP64.
+static bool block_has_fp32(const HostBlock& h) {
+  return coop_class(kPairClassL[h.cb][0], kPairClassL[h.cb][1], kPairClassL[h.ck][0],
+                    kPairClassL[h.ck][1]) < 0;
+}
+
 // Work list and build map of a full-tensor call (every unique quartet), made on first use.
 static int ensure_full_work(Basis& B) {
   if (B.d_work) return GBX_OK;
@@ -418,7 +480,7 @@ static int ensure_full_work(Basis& B) {
   for (int k = 0; k < nblk; ++k) {
     const HostBlock& h = B.blocks[k];
     bb[k] = BuildBlock{(int)B.class_first[h.cb], (int)h.nb, (int)B.class_first[h.ck], (int)h.nk,
-                       h.tri ? 1 : 0, k, h.dev.work_off, h.ncand};
+                       h.tri ? 1 : 0, k, h.dev.work_off, h.ncand, block_has_fp32(h) ? 1 : 0, 0};
     for (long long c0 = 0; c0 < h.ncand; c0 += 256) cmap.push_back(make_int2(k, (int)c0));
     if (h.ncand > (1LL << 31) - 256)
       return set_error(GBX_ERR_UNSUPPORTED, "class block with %lld quartets exceeds the limit",
@@ -511,27 +573,85 @@ int ensure_schwarz(Basis& B, cudaStream_t st) {
   }
   GBX_CUDA(cudaMemcpy(B.d_qscreen, B.h_q.data(), np * sizeof(double), cudaMemcpyHostToDevice),
            "upload screening bounds");
-  // bounds of the final values for the mixed form: segmented-pair bound times the largest
-  // output scale (norm_cont x component norm or sign) of each of its two shells
-  std::vector<double> smax(n, 0.0);
-  for (int i = 0; i < n; ++i)
-    for (int c = 0; c < kMaxCart; ++c) smax[i] = std::max(smax[i], std::fabs(B.shells[i].scl[c]));
-  std::vector<double> qm(np);
-  for (int p = 0; p < np; ++p) qm[p] = q[p] * smax[B.pairs[p].shA] * smax[B.pairs[p].shB];
-  if (!B.d_qmixed) {
-    const int s2 = B.alloc((void**)&B.d_qmixed, np * sizeof(double), "cudaMalloc(qmixed)");
-    if (s2) return s2;
-  }
-  GBX_CUDA(cudaMemcpy(B.d_qmixed, qm.data(), np * sizeof(double), cudaMemcpyHostToDevice),
-           "upload mixed bounds");
   B.schwarz_ready = true;
+  return GBX_OK;
+}
+
+// Q_p = sqrt(max |(ab|ab)|) over the output function pairs (a, b) of pair p, from the diagonal
+// entries of block (p, p) in the compact store.
+__global__ void diagonal_bounds(const PairDev* __restrict__ pairs, int npairs,
+                                const ShellDev* __restrict__ shells,
+                                const BlockDev* __restrict__ blocks,
+                                const double* __restrict__ compact, double* __restrict__ q) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const PairDev P = pairs[p];
+  const BlockDev b = blocks[P.cls * kNumPairClasses + P.cls];
+  const int nf = shells[P.shA].nout * P.nB;
+  double mx = 0.0;
+  for (int i = 0; i < nf; ++i) {
+    const long long r = (long long)P.fo + i;
+    mx = fmax(mx, fabs(compact[b.base + r * b.ncols + r]));
+  }
+  q[p] = sqrt(mx);
+}
+
+// Bounds of the final values for the mixed form: every output integral satisfies
+// |(ab|cd)| <= sqrt((ab|ab) (cd|cd)) <= Q_p Q_q (Cauchy-Schwarz for the output functions
+// themselves: norm_cont, component norms and spherical transforms included).  The diagonal
+// quartets (p, p) are computed by the class kernels into the compact store (scratch here:
+// the call that follows overwrites it).
+static int ensure_mixed_bounds(Basis& B, cudaStream_t st) {
+  if (B.mixed_ready) return GBX_OK;
+  int s;
+  const int np = (int)B.pairs.size();
+  if ((s = B.ensure_scratch(B.compact_elems, 0))) return s;
+  if (!B.d_qmixed && (s = B.alloc((void**)&B.d_qmixed, np * sizeof(double), "cudaMalloc(qmixed)")))
+    return s;
+  std::vector<int2> diag(np);
+  for (int p = 0; p < np; ++p) diag[p] = make_int2(p, p);
+  int2* d_diag = nullptr;
+  GBX_CUDA(cudaMalloc(&d_diag, np * sizeof(int2)), "cudaMalloc(diagonal quartets)");
+  cudaError_t e = cudaMemcpyAsync(d_diag, diag.data(), np * sizeof(int2), cudaMemcpyHostToDevice, st);
+  const int nsm = num_sms(B.device);
+  for (int c = 0; c < kNumPairClasses && e == cudaSuccess; ++c) {
+    if (B.class_count[c] == 0) continue;
+    const BlockDev& bd = B.block_table[(size_t)c * kNumPairClasses + c];
+    EriLaunch a = base_launch(B);
+    a.work = d_diag;
+    a.work_off = B.class_first[c];
+    a.nwork = B.class_count[c];
+    a.base = bd.base;
+    a.ncols = bd.ncols;
+    a.mode = 0;
+    a.team = 1;
+    const int grid = (int)std::min<long long>((a.nwork + 127) / 128, (long long)nsm * 8);
+    s = launch_class(kPairClassL[c][0], kPairClassL[c][1], kPairClassL[c][0], kPairClassL[c][1],
+                     a, std::max(grid, 1), st);
+    if (s) {
+      cudaStreamSynchronize(st);
+      cudaFree(d_diag);
+      return s;
+    }
+  }
+  if (e == cudaSuccess) {
+    diagonal_bounds<<<(np + 127) / 128, 128, 0, st>>>(B.d_pairs, np, B.d_shells, B.d_blocks,
+                                                      B.d_compact, B.d_qmixed);
+    e = cudaGetLastError();
+  }
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  cudaFree(d_diag);
+  GBX_CUDA(e, "mixed-form bounds");
+  GBX_CUDA(e2, "mixed-form bounds");
+  B.mixed_ready = true;
   return GBX_OK;
 }
 
 int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32) {
   int s;
   const bool mixed = skip > 0.0 || fp32 > 0.0;
-  if ((tau > 0.0 || mixed) && (s = ensure_schwarz(B, st))) return s;
+  if (tau > 0.0 && (s = ensure_schwarz(B, st))) return s;
+  if (mixed && (s = ensure_mixed_bounds(B, st))) return s;
   if ((s = ensure_full_work(B))) return s;
   if ((s = B.ensure_scratch(B.compact_elems, 0))) return s;
   const int nblk = (int)B.blocks.size();
@@ -590,7 +710,7 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
         (int)std::max<long long>(1, std::min<long long>((h.ncand * h.team + 127) / 128, (long long)nsm * 8));
     if (per_block) cudaEventRecord(B.blk_ev[i], st);
     if ((s = launch_class(la, lb, lc, ld, a, grid, bs))) return s;
-    if (mixed) {  // the block's FP32 list (the cooperative kernel runs it in FP64)
+    if (mixed && block_has_fp32(h)) {  // the block's FP32 list
       a.work_count = B.d_counts32 + k;
       a.reverse = 1;
       a.fp32 = 1;
@@ -712,6 +832,25 @@ ExpandArgs make_expand_args(const Basis& B, int notation, double* out) {
 
 int num_sms_of(int device) { return num_sms(device); }
 
+// Page-locked host staging ring of the pageable-output path, shared by the process (held
+// under g_pin_mu for the whole call that uses it) and kept for later calls.
+static std::mutex g_pin_mu;
+static double* g_pin_ring = nullptr;
+static size_t g_pin_elems = 0;
+
+static int ensure_pinned_ring(size_t elems, double** ring) {
+  if (g_pin_elems < elems) {
+    if (g_pin_ring) cudaFreeHost(g_pin_ring);
+    g_pin_ring = nullptr;
+    g_pin_elems = 0;
+    GBX_CUDA(cudaHostAlloc((void**)&g_pin_ring, elems * sizeof(double), cudaHostAllocPortable),
+             "cudaHostAlloc(staging ring)");
+    g_pin_elems = elems;
+  }
+  *ring = g_pin_ring;
+  return GBX_OK;
+}
+
 // Full tensor into host memory without an N^4 device buffer: after the class kernels, the
 // tensor is expanded slab by slab (x-ranges of out[x, ...], each a contiguous host range)
 // into kStageBuffers device staging slabs; each slab is copied out on a copy stream while
@@ -756,9 +895,24 @@ int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStre
   if ((s = run_compact(B, tau, st))) return s;
   const ExpandArgs e = expand_args(B, notation, nullptr);
   const int nsm = num_sms(B.device);
-  int i = 0;
-  for (long long x0 = 0; x0 < n; x0 += xs, ++i) {
-    const long long x1 = std::min(n, x0 + xs);
+  const int nslab = (int)((n + xs - 1) / xs);
+  // page-locked destination: slabs are copied straight into it; pageable: through a
+  // page-locked staging ring, from which host threads copy each slab into place
+  bool pinned = true;
+  for (const double* p : {out_host, out_host + (size_t)n * slab - 1}) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess || at.type != cudaMemoryTypeHost)
+      pinned = false;
+  }
+  cudaGetLastError();
+  std::unique_lock<std::mutex> pin_lock;
+  double* hring = nullptr;
+  if (!pinned) {
+    pin_lock = std::unique_lock<std::mutex>(g_pin_mu);
+    if ((s = ensure_pinned_ring(kStageBuffers * chunk, &hring))) return s;
+  }
+  auto issue = [&](int i) -> int {
+    const long long x0 = (long long)i * xs, x1 = std::min(n, x0 + xs);
     const int k = i % kStageBuffers;
     double* buf = B.d_stage + (size_t)k * B.stage_elems;
     if (i >= kStageBuffers) GBX_CUDA(cudaStreamWaitEvent(st, B.stage_free[k], 0), "wait slab");
@@ -768,11 +922,57 @@ int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStre
     GBX_CUDA(cudaGetLastError(), "expand_slab launch");
     GBX_CUDA(cudaEventRecord(B.stage_ready[k], st), "record slab");
     GBX_CUDA(cudaStreamWaitEvent(B.copy_stream, B.stage_ready[k], 0), "wait slab");
-    GBX_CUDA(cudaMemcpyAsync(out_host + (size_t)x0 * slab, buf,
-                             (size_t)(x1 - x0) * slab * sizeof(double), cudaMemcpyDeviceToHost,
-                             B.copy_stream),
+    double* dst = pinned ? out_host + (size_t)x0 * slab : hring + (size_t)k * chunk;
+    GBX_CUDA(cudaMemcpyAsync(dst, buf, (size_t)(x1 - x0) * slab * sizeof(double),
+                             cudaMemcpyDeviceToHost, B.copy_stream),
              "copy slab to host");
     GBX_CUDA(cudaEventRecord(B.stage_free[k], B.copy_stream), "record slab copy");
+    return GBX_OK;
+  };
+  if (pinned) {
+    for (int i = 0; i < nslab; ++i)
+      if ((s = issue(i))) return s;
+  } else {
+    // workers copy their share of each slab once its device-to-host copy has finished; slab
+    // i + kStageBuffers reuses ring slot i % kStageBuffers only after every worker is done
+    const int nthr = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency() / 2));
+    std::atomic<int> issued{0}, failed{0};
+    std::unique_ptr<std::atomic<int>[]> done(new std::atomic<int>[nslab]);
+    for (int i = 0; i < nslab; ++i) done[i].store(0);
+    auto worker = [&](int t) {
+      for (int i = 0; i < nslab; ++i) {
+        while (issued.load(std::memory_order_acquire) <= i) {
+          if (failed.load()) return;
+          std::this_thread::yield();
+        }
+        if (cudaEventSynchronize(B.stage_free[i % kStageBuffers]) != cudaSuccess) {
+          failed.store(1);
+        } else {
+          const long long x0 = (long long)i * xs, x1 = std::min(n, x0 + xs);
+          const size_t len = (size_t)(x1 - x0) * slab;
+          const size_t a = len * t / nthr, b = len * (t + 1) / nthr;
+          std::memcpy(out_host + (size_t)x0 * slab + a,
+                      hring + (size_t)(i % kStageBuffers) * chunk + a, (b - a) * sizeof(double));
+        }
+        done[i].fetch_add(1, std::memory_order_release);
+      }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthr; ++t) pool.emplace_back(worker, t);
+    for (int i = 0; i < nslab && !s; ++i) {
+      if (i >= kStageBuffers)
+        while (done[i - kStageBuffers].load(std::memory_order_acquire) < nthr) {
+          if (failed.load()) break;
+          std::this_thread::yield();
+        }
+      if (failed.load()) break;
+      s = issue(i);
+      if (!s) issued.store(i + 1, std::memory_order_release);
+    }
+    if (s) failed.store(1);
+    for (std::thread& th : pool) th.join();
+    if (s) return s;
+    if (failed.load()) return set_error(GBX_ERR_CUDA, "slab copy to host failed");
   }
   GBX_CUDA(cudaStreamSynchronize(B.copy_stream), "synchronize copies");
   GBX_CUDA(cudaStreamSynchronize(st), "synchronize");
@@ -804,6 +1004,34 @@ int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, d
   }
   if (B.profiling) cudaEventRecord(B.ev[3], st);
   return GBX_OK;
+}
+
+int unique_values(Basis& B, long long n, const long long* idx4_host, double* out_host,
+                  cudaStream_t st) {
+  if (!B.d_compact) return set_error(GBX_ERR_INVALID, "no integrals computed on this basis yet");
+  for (long long i = 0; i < 4 * n; ++i)
+    if (idx4_host[i] < 0 || idx4_host[i] >= B.nbf)
+      return set_error(GBX_ERR_INVALID, "function index %lld out of range [0, %lld)",
+                       (long long)idx4_host[i], B.nbf);
+  if (n == 0) return GBX_OK;
+  long long* d_idx = nullptr;
+  double* d_out = nullptr;
+  GBX_CUDA(cudaMalloc(&d_idx, (size_t)n * 4 * sizeof(long long)), "cudaMalloc(indices)");
+  cudaError_t err = cudaMalloc(&d_out, (size_t)n * sizeof(double));
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(d_idx, idx4_host, (size_t)n * 4 * sizeof(long long),
+                          cudaMemcpyHostToDevice, st);
+  if (err == cudaSuccess) {
+    gather_unique<<<(int)((n + 255) / 256), 256, 0, st>>>(expand_args(B, GBX_CHEMIST, nullptr),
+                                                        d_idx, n, d_out);
+    err = cudaGetLastError();
+  }
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(out_host, d_out, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+  cudaFree(d_idx);
+  if (d_out) cudaFree(d_out);
+  return cuda_status(err, "unique values");
 }
 
 }  // namespace gbx

@@ -9,6 +9,8 @@ struct BuildBlock {
   int pb0, nb, pk0, nk;
   int tri, blk;
   long long work_off, ncand;
+  int fp32_ok;  // the block's class kernel has an FP32 path (mixed form); 0: FP64 only
+  int pad;
 };
 
 // Full-tensor expansion (K6).

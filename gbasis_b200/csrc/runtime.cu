@@ -451,6 +451,24 @@ int gbx_eri_unique(gbx_basis* b, double skip, double fp32, void* stream) {
   return run_compact(B, 0.0, (cudaStream_t)stream, skip, fp32);
 }
 
+int gbx_compact_view(gbx_basis* b, const double** dev_ptr, int64_t* n_elems) {
+  if (!b || !dev_ptr || !n_elems) return set_error(GBX_ERR_INVALID, "gbx_compact_view: null argument");
+  const Basis& B = *b->impl;
+  *dev_ptr = B.d_compact;
+  *n_elems = B.d_compact ? B.compact_elems : 0;
+  return GBX_OK;
+}
+
+int gbx_unique_values(gbx_basis* b, int64_t n, const int64_t* idx4, double* out_host,
+                      void* stream) {
+  if (!b || n < 0 || (n > 0 && (!idx4 || !out_host)))
+    return set_error(GBX_ERR_INVALID, "gbx_unique_values: null argument");
+  Basis& B = *b->impl;
+  DeviceGuard g(B.device);
+  return unique_values(B, n, reinterpret_cast<const long long*>(idx4), out_host,
+                       (cudaStream_t)stream);
+}
+
 int gbx_eri_full_host(gbx_basis* b, int notation, double tau, double* out_host, void* stream) {
   if (!b || !out_host) return set_error(GBX_ERR_INVALID, "gbx_eri_full_host: null argument");
   if (notation != GBX_CHEMIST && notation != GBX_PHYSICIST)

@@ -78,6 +78,7 @@ struct Basis {
   double* d_out = nullptr;
   size_t out_cap = 0;
   bool schwarz_ready = false;
+  bool mixed_ready = false;  // d_qmixed holds the final-value bounds
   std::vector<double> h_q;  // per pair, original-shell-pair bound
   long long last_computed = 0, last_screened = 0;
   // optional phase timing with events on the launching stream:
@@ -115,6 +116,8 @@ int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStre
 int run_compact(Basis& B, double tau, cudaStream_t st, double skip = 0.0, double fp32 = 0.0);
 int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st);
 int ensure_schwarz(Basis& B, cudaStream_t st);
+int unique_values(Basis& B, long long n, const long long* idx4_host, double* out_host,
+                  cudaStream_t st);
 struct ExpandArgs;
 int launch_expand_batch(int device, const ExpandArgs* d_mols, const long long* d_row_first,
                         int nmol, long long total_rows, size_t max_row_bytes, cudaStream_t st);

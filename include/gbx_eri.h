@@ -99,6 +99,15 @@ int gbx_eri_full_mixed(gbx_basis* b, int notation, double skip, double fp32, dou
  * integral work of a full call, for bases whose full tensor does not fit in memory.
  * skip = fp32 = 0 is the FP64 form. */
 int gbx_eri_unique(gbx_basis* b, double skip, double fp32, void* stream);
+/* (ab|cd) in the output functions of the basis for n quadruples idx4[4i..4i+3] = (a,b,c,d),
+ * read from the compact store of the last gbx_eri_unique / gbx_eri_full* call on b (the
+ * values that call produced, mixed form included) into host memory; synchronous. */
+int gbx_unique_values(gbx_basis* b, int64_t n, const int64_t* idx4, double* out_host,
+                      void* stream);
+/* Device address and length (doubles) of the compact store holding the last call's unique
+ * integrals (class blocks of pair functions; NULL / 0 before the first call).  Read-only,
+ * valid until the next call on b; for whole-store comparisons such as mixed vs FP64. */
+int gbx_compact_view(gbx_basis* b, const double** dev_ptr, int64_t* n_elems);
 /* Same as gbx_eri_full, into host memory (page-locked or pageable); synchronous. */
 int gbx_eri_full_host(gbx_basis* b, int notation, double schwarz_threshold, double* out_host,
                       void* stream);
