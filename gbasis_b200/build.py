@@ -46,11 +46,16 @@ def sources(lmax):
 
 KERNEL_DEPS = ("gbx_common.cuh", "eri_kernels.cuh", "errors.h", "_gen/eri_gen.cuh")
 HOST_DEPS = ("gbx_common.cuh", "runtime.h", "errors.h", "pipeline_kernels.cuh", "coop.cuh",
-             "_gen/coop_programs.cuh")
+             "coop_tail.cuh", "_gen/coop_programs.cuh")
+
+
+LINES_DEPS = ("gbx_common.cuh", "errors.h", "coop.cuh", "coop_tail.cuh", "lines_kernel.cuh")
 
 
 def _deps_mtime(src):
-    deps = KERNEL_DEPS if os.path.basename(src).startswith("eri_cls") else HOST_DEPS
+    base = os.path.basename(src)
+    deps = (KERNEL_DEPS if base.startswith("eri_cls") else
+            LINES_DEPS if base.startswith("lines_") else HOST_DEPS)
     m = os.path.getmtime(os.path.join(ROOT, "include", "gbx_eri.h"))
     for d in deps:
         p = os.path.join(CSRC, d)

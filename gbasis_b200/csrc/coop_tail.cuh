@@ -1,0 +1,331 @@
+// Shared pieces of the cooperative (warp-per-quartet) kernels: launch arguments, the Boys
+// evaluation by lanes, and the per-quartet tail (phases B-D: ket HRR, ket Cartesian->spherical
+// transform, bra HRR + transform, permutation/scale and store, Schwarz or Coulomb epilogues)
+// that runs once the contracted [e0|f0] are in shared memory ACC.  Included after a
+// translation unit's recursion-program tables (kCoopIns, kCoopLv, kCoopIdx, kCoopSph, kCoopCn).
+// Mathematics: gbasis/integrals/_two_elec_int.py:549-812 (HRR, component norm) and
+// gbasis/base_four_symm.py:195-349 (norm_cont, spherical transform).
+#pragma once
+#include <algorithm>
+
+#include "coop.cuh"
+#include "errors.h"
+
+namespace gbx {
+
+struct CoopArgs {
+  EriLaunch a;
+  CoopMeta m;
+  int R, Cc, smem_per_warp;  // rows / columns per HRR chunk, doubles of smem per warp
+  int prog_doubles;          // shared memory taken by the staged programs (0: read globally)
+  int extra_doubles = 0;     // per-CTA shared memory after the programs (line kernel: Boys table)
+};
+
+constexpr long long kCoopMaxSmem = 227 * 1024;
+
+// Shared-memory plan of a cooperative launch.  Per warp: ACC (NE*NF) followed by the larger
+// of phase A's `phase_a` doubles and the tail's buffers (rows R and columns Cc per HRR chunk,
+// halved until a warp fits 48 KB); the class's programs are staged once per CTA when they fit;
+// up to 4 warps per CTA.
+inline int coop_plan(const CoopMeta& M, long long phase_a, CoopArgs& A, size_t& smem, int& wpc) {
+  const int NCD = ncart(M.lc) * ncart(M.ld), NAB = ncart(M.la) * ncart(M.lb);
+  const int NENF = M.NE * M.NF;
+  const long long budget = 48 * 1024 / 8;
+  auto size_for = [&](int R, int Cc) {
+    long long s = NENF + phase_a;
+    s = std::max<long long>(s, NENF + (long long)M.NE * NCD + (long long)R * M.nK);
+    s = std::max<long long>(s, NENF + (long long)M.NE * NCD + NCD);
+    s = std::max<long long>(s, NENF + (long long)M.NE * NCD + (long long)Cc * (M.nB + 2 * NAB) +
+                                   2 * NAB);
+    return s;
+  };
+  int R = 8, Cc = 8;
+  while ((R > 1 || Cc > 1) && size_for(R, Cc) > budget) {
+    if (R > 1) R /= 2;
+    if (Cc > 1) Cc /= 2;
+  }
+  A.R = R;
+  A.Cc = Cc;
+  const long long per_warp = size_for(R, Cc);
+  A.smem_per_warp = (int)per_warp;
+  const long long prog_bytes = (long long)M.n_ins * 16 + (long long)M.n_idx * 2;
+  const long long extra = (long long)A.extra_doubles * 8;
+  A.prog_doubles = 0;
+  if (prog_bytes <= 32 * 1024 && prog_bytes + extra + per_warp * 8 <= kCoopMaxSmem)
+    A.prog_doubles = (int)((prog_bytes + 15) / 16 * 2);
+  const long long avail = kCoopMaxSmem - (long long)A.prog_doubles * 8 - extra;
+  wpc = (int)std::max<long long>(1, std::min<long long>(4, avail / (per_warp * 8)));
+  smem = (size_t)A.prog_doubles * 8 + (size_t)extra + (size_t)wpc * per_warp * 8;
+  if ((long long)smem > kCoopMaxSmem)
+    return set_error(GBX_ERR_UNSUPPORTED, "class (%d%d|%d%d) needs %zu bytes of shared memory",
+                     M.la, M.lb, M.lc, M.ld, smem);
+  return GBX_OK;
+}
+
+inline int coop_grid(const EriLaunch& a, int wpc) {
+  int dev = 0, nsm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  return (int)std::max<long long>(1, std::min<long long>((a.nwork + wpc - 1) / wpc, (long long)nsm * 8));
+}
+
+// Access to a class's programs, staged in shared memory or read from the global tables.
+struct ProgView {
+  const short (*ins)[8];
+  const short* idx;
+  int ins0, idx0;
+  __device__ __forceinline__ const short* I(int i) const { return ins[i - ins0]; }
+  __device__ __forceinline__ int X(int j) const { return idx[j - idx0]; }
+};
+
+__device__ __forceinline__ double pick3(int d, double x, double y, double z) {
+  return d == 0 ? x : (d == 1 ? y : z);
+}
+
+__device__ __forceinline__ const double* sph_mat(int l) { return kCoopSph + (l == 2 ? 0 : 30); }
+
+__device__ __forceinline__ int n_int(const ShellDev& s) {
+  return (s.sph && s.l >= 2) ? 2 * s.l + 1 : ncart(s.l);
+}
+
+// Lane m <= L writes pref * F_m(T) to X[m]: T < 40 by the 8-term Taylor expansion of F_m
+// around the nearest grid point (orders m..m+7 of the table), T >= 40 by F_0 = sqrt(pi/T)/2
+// and m upward steps F_{k+1} = ((2k+1) F_k - e^{-T})/(2T).
+__device__ __forceinline__ void boys_lanes(int L, int lane, double T, double pref,
+                                           const double* __restrict__ tab, double* X) {
+  if (lane > L) return;
+  double f;
+  if (T < kBoysTMax) {
+    const int n = __double2int_rn(T * 10.0);
+    const double x = fma(-T, 10.0, (double)n) * 0.1;
+    const double* g = tab + n * (kBoysOrders + 1) + lane;
+    f = g[7] * (1.0 / 5040);
+    f = fma(f, x, g[6] * (1.0 / 720));
+    f = fma(f, x, g[5] * (1.0 / 120));
+    f = fma(f, x, g[4] * (1.0 / 24));
+    f = fma(f, x, g[3] * (1.0 / 6));
+    f = fma(f, x, g[2] * 0.5);
+    f = fma(f, x, g[1]);
+    f = fma(f, x, g[0]);
+  } else {
+    const double r = rsqrt(T);
+    f = 0.88622692545275801365 * r;
+    if (lane > 0) {
+      const double emT = exp(-T), o2T = 0.5 * r * r;
+      for (int m = 0; m < lane; ++m) f = fma((double)(2 * m + 1), f, -emT) * o2T;
+    }
+  }
+  X[lane] = f * pref;
+}
+
+// Phases B-D of one quartet (bra pair pq.x, ket pair pq.y) from ACC = S[0 .. NE*NF).
+__device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv, double* S,
+                                          const int2 pq, const PairDev& P, const PairDev& Q,
+                                          const int lane) {
+  const EriLaunch& a = A.a;
+  const CoopMeta& M = A.m;
+  auto INS = [&](int i) -> const short* { return pv.I(i); };
+  auto IDX = [&](int j) -> int { return pv.X(j); };
+  const int NENF = M.NE * M.NF;
+  const int NCA = ncart(M.la), NCB = ncart(M.lb), NCC = ncart(M.lc), NCDD = ncart(M.ld);
+  const int NCD = NCC * NCDD, NAB = NCA * NCB;
+  double* ACC = S;
+  double* HF = S + NENF;
+  double* KN = HF + M.NE * NCD;
+  double* T1 = KN;
+  double* BN = KN;
+  double* OB = BN + A.Cc * M.nB;
+  double* T2 = OB + A.Cc * NAB;
+  double* VAB = T2 + A.Cc * NAB;  // Coulomb mode: sum_cd (ab|cd) D[c][d] per (a, b)
+  double* DAB = VAB + NAB;        // Coulomb mode: D[a][b] of the bra block
+    // ---------------------------------------------------------------- B
+  // HF[e][cd] overlays X (dead); rows are processed R at a time in KN
+  for (int r0 = 0; r0 < M.NE; r0 += A.R) {
+    const int rr = min(A.R, M.NE - r0);
+    for (int i = lane; i < rr * M.NF; i += 32) {
+      const int r = i / M.NF, f = i - r * M.NF;
+      KN[r * M.nK + f] = ACC[(r0 + r) * M.NF + f];
+    }
+    __syncwarp();
+    for (int l = 0; l < M.k_nlv; ++l) {
+      const int b = kCoopLv[M.k_lv + l], e = kCoopLv[M.k_lv + l + 1], cnt = e - b;
+      for (int i = lane; i < rr * cnt; i += 32) {
+        const int r = i / cnt;
+        const short* I = INS(M.k_ins + b + (i - r * cnt));
+        double* Kr = KN + r * M.nK;
+        Kr[I[0]] = fma(pick3(I[5], Q.ABx, Q.ABy, Q.ABz), Kr[I[2]], Kr[I[1]]);
+      }
+      __syncwarp();
+    }
+    for (int i = lane; i < rr * NCD; i += 32) {
+      const int r = i / NCD, j = i - r * NCD;
+      HF[(r0 + r) * NCD + j] = KN[r * M.nK + IDX(M.kfin + j)];
+    }
+    __syncwarp();
+  }
+  const ShellDev& sA = a.shells[P.shA];
+  const ShellDev& sB = a.shells[P.shB];
+  const ShellDev& sC = a.shells[Q.shA];
+  const ShellDev& sD = a.shells[Q.shB];
+  const bool schwarz = a.mode == 1;  // Cartesian block, max |(ab|ab)| with component norms
+  const bool coulomb = a.mode == 2;  // accumulate J instead of storing the block
+  const int nAi = schwarz ? NCA : n_int(sA), nBi = schwarz ? NCB : n_int(sB);
+  const int nCi = schwarz ? NCC : n_int(sC), nDi = schwarz ? NCDD : n_int(sD);
+  double mx = 0.0;
+  if (coulomb) {
+    for (int i = lane; i < nAi * nBi; i += 32) {
+      const int ua = i / nBi, ub = i - ua * nBi;
+      VAB[i] = 0.0;
+      DAB[i] = a.D[(sA.func_off + sA.pos[ua]) * a.nbf + sB.func_off + sB.pos[ub]] *
+               sA.scl[ua] * sB.scl[ub];
+    }
+    __syncwarp();
+  }
+  // ---------------------------------------------------------------- C
+  if (nCi != NCC || nDi != NCDD) {
+    for (int e = 0; e < M.NE; ++e) {
+      double* row = HF + e * NCD;
+      // axis D: T1[c][ud]
+      for (int i = lane; i < NCC * nDi; i += 32) {
+        const int c = i / nDi, ud = i - c * nDi;
+        double v;
+        if (nDi != NCDD) {
+          const double* W = sph_mat(M.ld) + ud * NCDD;
+          v = 0.0;
+          for (int d = 0; d < NCDD; ++d) v = fma(W[d], row[c * NCDD + d], v);
+        } else {
+          v = row[c * NCDD + ud];
+        }
+        T1[i] = v;
+      }
+      __syncwarp();
+      // axis C: row[uc * nDi + ud]
+      for (int i = lane; i < nCi * nDi; i += 32) {
+        const int uc = i / nDi, ud = i - uc * nDi;
+        double v;
+        if (nCi != NCC) {
+          const double* W = sph_mat(M.lc) + uc * NCC;
+          v = 0.0;
+          for (int c = 0; c < NCC; ++c) v = fma(W[c], T1[c * nDi + ud], v);
+        } else {
+          v = T1[uc * nDi + ud];
+        }
+        row[i] = v;
+      }
+      __syncwarp();
+    }
+  }
+  // ---------------------------------------------------------------- D
+  const int ncol = nCi * nDi;
+  const long long nBo = sB.nout, nDo = sD.nout;
+  long long bbase, bcols;
+  block_dest(a, P, bbase, bcols);
+  double* __restrict__ dst = a.out + bbase + Q.fo;
+  for (int c0 = 0; c0 < ncol; c0 += A.Cc) {
+    const int cc = min(A.Cc, ncol - c0);
+    for (int i = lane; i < cc * M.NE; i += 32) {
+      const int c = i / M.NE, e = i - c * M.NE;
+      BN[c * M.nB + e] = HF[e * NCD + c0 + c];
+    }
+    __syncwarp();
+    for (int l = 0; l < M.b_nlv; ++l) {
+      const int b = kCoopLv[M.b_lv + l], e = kCoopLv[M.b_lv + l + 1], cnt = e - b;
+      for (int i = lane; i < cc * cnt; i += 32) {
+        const int c = i / cnt;
+        const short* I = INS(M.b_ins + b + (i - c * cnt));
+        double* Bc = BN + c * M.nB;
+        Bc[I[0]] = fma(pick3(I[5], P.ABx, P.ABy, P.ABz), Bc[I[2]], Bc[I[1]]);
+      }
+      __syncwarp();
+    }
+    for (int i = lane; i < cc * NAB; i += 32) {
+      const int c = i / NAB, j = i - c * NAB;
+      OB[i] = BN[c * M.nB + IDX(M.bfin + j)];
+    }
+    __syncwarp();
+    // axis B then A (per column), result in OB as [c][ua][ub] with row stride nBi
+    if (nBi != NCB) {
+      const double* W = sph_mat(M.lb);
+      for (int i = lane; i < cc * NCA * nBi; i += 32) {
+        const int c = i / (NCA * nBi), rem = i - c * NCA * nBi, a_ = rem / nBi, ub = rem - a_ * nBi;
+        double v = 0.0;
+        for (int b = 0; b < NCB; ++b) v = fma(W[ub * NCB + b], OB[c * NAB + a_ * NCB + b], v);
+        T2[c * NAB + a_ * nBi + ub] = v;
+      }
+    } else {
+      for (int i = lane; i < cc * NAB; i += 32) T2[i] = OB[i];
+    }
+    __syncwarp();
+    if (nAi != NCA) {
+      const double* W = sph_mat(M.la);
+      for (int i = lane; i < cc * nAi * nBi; i += 32) {
+        const int c = i / (nAi * nBi), rem = i - c * nAi * nBi, ua = rem / nBi, ub = rem - ua * nBi;
+        double v = 0.0;
+        for (int a_ = 0; a_ < NCA; ++a_) v = fma(W[ua * NCA + a_], T2[c * NAB + a_ * nBi + ub], v);
+        OB[c * NAB + ua * nBi + ub] = v;
+      }
+    } else {
+      for (int i = lane; i < cc * NAB; i += 32) OB[i] = T2[i];
+    }
+    __syncwarp();
+    if (coulomb) {
+      // J[a][b] partial sums over this chunk's columns; J[c][d] of each column
+      const int nab = nAi * nBi;
+      for (int i = lane; i < nab; i += 32) {
+        double s = VAB[i];
+        for (int c = 0; c < cc; ++c) {
+          const int col = c0 + c, uc = col / nDi, ud = col - uc * nDi;
+          const double dcd = a.D[(sC.func_off + sC.pos[uc]) * a.nbf + sD.func_off + sD.pos[ud]] *
+                             sC.scl[uc] * sD.scl[ud];
+          s = fma(OB[c * NAB + i], dcd, s);
+        }
+        VAB[i] = s;
+      }
+      if (pq.x != pq.y) {
+        for (int c = lane; c < cc; c += 32) {
+          const int col = c0 + c, uc = col / nDi, ud = col - uc * nDi;
+          double s = 0.0;
+          for (int i = 0; i < nab; ++i) s = fma(OB[c * NAB + i], DAB[i], s);
+          s *= ((P.shA != P.shB) ? 2.0 : 1.0) * sC.scl[uc] * sD.scl[ud];
+          const long long fc = sC.func_off + sC.pos[uc], fd = sD.func_off + sD.pos[ud];
+          atomicAdd(a.J + fc * a.nbf + fd, s);
+          if (Q.shA != Q.shB) atomicAdd(a.J + fd * a.nbf + fc, s);
+        }
+      }
+      __syncwarp();
+      continue;
+    }
+    for (int i = lane; i < cc * nAi * nBi; i += 32) {
+      const int c = i / (nAi * nBi), rem = i - c * nAi * nBi, ua = rem / nBi, ub = rem - ua * nBi;
+      const int col = c0 + c, uc = col / nDi, ud = col - uc * nDi;
+      if (schwarz) {
+        mx = fmax(mx, fabs(OB[c * NAB + ua * nBi + ub]) * kCoopCn[M.la * 10 + ua] *
+                          kCoopCn[M.lb * 10 + ub] * kCoopCn[M.lc * 10 + uc] *
+                          kCoopCn[M.ld * 10 + ud]);
+        continue;
+      }
+      const double v = OB[c * NAB + ua * nBi + ub] * sA.scl[ua] * sB.scl[ub] * sC.scl[uc] *
+                       sD.scl[ud];
+      dst[((long long)P.fo + sA.pos[ua] * nBo + sB.pos[ub]) * bcols + sC.pos[uc] * nDo +
+          sD.pos[ud]] = v;
+    }
+    __syncwarp();
+  }
+  if (schwarz) {
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) a.qout[pq.x] = sqrt(mx);
+  }
+  if (coulomb) {
+    const double fk = (Q.shA != Q.shB) ? 2.0 : 1.0;
+    for (int i = lane; i < nAi * nBi; i += 32) {
+      const int ua = i / nBi, ub = i - ua * nBi;
+      const long long fa = sA.func_off + sA.pos[ua], fbn = sB.func_off + sB.pos[ub];
+      const double s = VAB[i] * fk * sA.scl[ua] * sB.scl[ub];
+      atomicAdd(a.J + fa * a.nbf + fbn, s);
+      if (P.shA != P.shB) atomicAdd(a.J + fbn * a.nbf + fa, s);
+    }
+  }
+  __syncwarp();
+}
+
+}  // namespace gbx

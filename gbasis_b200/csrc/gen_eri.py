@@ -427,7 +427,12 @@ def emit_sources(outdir, lmax):
         name = f"eri_cls_{k:02d}.cu"
         put(name, "\n".join(lines) + "\n")
         files.append(name)
+    import gen_lines
+    lfiles, launchers = gen_lines.emit_sources(outdir, heavy)
+    files += lfiles
     lines = ["// Generated by gen_eri.py: (la,lb,lc,ld) -> class kernel launcher.",
+             "#include <cstdlib>",
+             "#include <cstring>",
              '#include "../coop.cuh"',
              '#include "../runtime.h"',
              "namespace gbx {",
@@ -436,6 +441,15 @@ def emit_sources(outdir, lmax):
     for c in light:
         lines.append(f"extern template int launch_t<{c[0]}, {c[1]}, {c[2]}, {c[3]}>(const EriLaunch&, "
                      "int, cudaStream_t);")
+    for c in heavy:
+        lines.append(f"int {launchers[c]}(const EriLaunch& a, cudaStream_t st);")
+    lines.append("// Heavy classes run the line-factorised kernel; GBX_HEAVY_KERNEL=interp selects the")
+    lines.append("// program-interpreting cooperative kernel instead (read once per process).")
+    lines.append("static bool heavy_interp() {")
+    lines.append('  static const bool v = [] { const char* e = std::getenv("GBX_HEAVY_KERNEL");')
+    lines.append('                             return e && std::strcmp(e, "interp") == 0; }();')
+    lines.append("  return v;")
+    lines.append("}")
     lines.append(f"int compiled_lmax() {{ return {lmax}; }}")
     lines.append("int launch_class(int la, int lb, int lc, int ld, const EriLaunch& a, int grid, "
                  "cudaStream_t st) {")
@@ -445,7 +459,8 @@ def emit_sources(outdir, lmax):
         lines.append(f"    case {key}: return launch_t<{c[0]}, {c[1]}, {c[2]}, {c[3]}>(a, grid, st);")
     for j, c in enumerate(heavy):
         key = ((c[0] * 8 + c[1]) * 8 + c[2]) * 8 + c[3]
-        lines.append(f"    case {key}: return launch_coop({j}, a, st);")
+        lines.append(f"    case {key}: return heavy_interp() ? launch_coop({j}, a, st) : "
+                     f"{launchers[c]}(a, st);")
     lines.append("    default: break;")
     lines.append("  }")
     lines.append('  return set_error(GBX_ERR_UNSUPPORTED, "no kernel for class (%d %d|%d %d)", '

@@ -1,0 +1,431 @@
+// Line-factorised cooperative ERI kernel for heavy classes: one warp per contracted quartet.
+//
+// Every step of the Obara-Saika vertical recursion and of the electron transfer couples
+// neighbours along one Cartesian axis only (the step direction is z if that component is
+// non-zero, else y, else x), so a primitive quartet splits into stages of independent 1-D
+// lines, each run by one lane in registers:
+//   vrr_xy  lane e_x:          [(ex,0,0)]^(m) by x steps, then [(ex,ey,0)]^(m) by y steps -> Y
+//   vrr_z   line (ex,ey):      [(ex,ey,ez)]^(0) by z steps                              -> W(0,0)
+//   etr_x   line (ey,ez):      table (ex, fx): [e,(fx,0,0)]                             -> W(fx,0)
+//   etr_y   line (ex,ez), fx:  table (ey, fy): [e,(fx,fy,0)]                            -> W(fx,fy)
+//   etr_z   line (ex,ey,fx,fy): table (ez, fz): [e,f], targets added to ACC[e][f]
+// Values cross shared memory once between stages.  W is a set of tetrahedral blocks, one per
+// (fx, fy): element (ex,ey,ez) of block (fx,fy) sits at zb(fx,fy) + toff(ex,ey,g) + ez with
+// g = L - fx - fy; Y has the layout of block (0,0) with m in place of ez.  Lines come in
+// rounds of 32 (one per lane, generated tables); a round's code is unrolled to its largest
+// extent NMAX and each lane predicates its own cells.
+//
+// Recursions (gbasis/integrals/_two_elec_int.py:350-526):
+//   [e+1_i]^(m) = PA_i [e]^(m) + WP_i [e]^(m+1) + e_i/(2 zeta) ([e-1_i]^(m) - rho/zeta [e-1_i]^(m+1))
+//   [e, f+1_i] = CE_i [e,f] + e_i/(2 eta) [e-1_i,f] + f_i/(2 eta) [e,f-1_i] - zeta/eta [e+1_i,f]
+#pragma once
+#include "coop_tail.cuh"
+#include "eri_kernels.cuh"  // sph_axis, gen::Sph, gen::cnorm
+
+namespace gbx {
+
+__host__ __device__ constexpr int lines_tet(int k) { return k * (k + 1) * (k + 2) / 6; }
+
+// Offset of (ex, ey, 0) in a tetrahedral block of extent g (ex + ey + ez <= g).
+__host__ __device__ constexpr int lines_toff(int ex, int ey, int g) {
+  return lines_tet(g + 1) - lines_tet(g + 1 - ex) + ey * (g + 1 - ex) - ey * (ey - 1) / 2;
+}
+
+// Start of W block (fx, fy): blocks in order fx = 0..F, fy = 0..F-fx.
+__host__ __device__ constexpr int lines_zb(int L, int F, int fx, int fy) {
+  int off = 0;
+  for (int a = 0; a <= F; ++a)
+    for (int b = 0; b <= F - a; ++b) {
+      if (a == fx && b == fy) return off;
+      off += lines_tet(L - a - b + 1);
+    }
+  return off;
+}
+
+struct LinePS {
+  double PAx, PAy, PAz, WPx, WPy, WPz, CEx, CEy, CEz;
+  double o2z, rz, ze, o2e;
+};
+
+// One step of the vertical recursion along an axis: c holds [k-1]^(m), p holds [k-2]^(m);
+// afterwards c holds [k]^(m) for m <= M - k and p holds the old c.
+template <int M>
+__device__ __forceinline__ void lines_vstep(double* c, double* p, int k, double PA, double WP,
+                                            double o2z, double rz) {
+  const double a = (double)(k - 1) * o2z;
+#pragma unroll
+  for (int m = 0; m <= M; ++m) {
+    if (m <= M - k) {
+      double v = fma(PA, c[m], WP * c[m + 1]);
+      v = fma(a, fma(-rz, p[m + 1], p[m]), v);
+      p[m] = c[m];
+      c[m] = v;
+    }
+  }
+}
+
+// One transfer step along an axis over a line's cells a <= M: r1 = [.., f] (cells a), r0 =
+// [.., f - 1_i]; k = f_i of f.  Result cell a = CE r1[a] - ze r1[a+1] + a/(2 eta) r1[a-1]
+// + k/(2 eta) r0[a]; r0 <- r1, r1 <- result.
+template <int M>
+__device__ __forceinline__ void lines_tstep(double* r1, double* r0, int k, int ext, double CE,
+                                            double ze, double o2e, int lim) {
+  // cells a <= lim (a compile-time bound at every unrolled call site); the rest stay zero
+  double nw[M + 1];
+  const double kk = (double)k * o2e;
+#pragma unroll
+  for (int a = 0; a <= M; ++a) {
+    if (a <= lim) {
+      double v = fma(CE, r1[a], -ze * r1[a + 1]);
+      if (a >= 1) v = fma((double)a * o2e, r1[a - 1], v);
+      v = fma(kk, r0[a], v);
+      nw[a] = (a <= ext) ? v : 0.0;
+    } else {
+      nw[a] = 0.0;
+    }
+  }
+#pragma unroll
+  for (int a = 0; a <= M; ++a) {
+    r0[a] = r1[a];
+    r1[a] = nw[a];
+  }
+}
+
+// VRR along x then y; lane ex <= L writes Y[toff(ex, ey, L) + m] = [(ex,ey,0)]^(m).
+template <int L>
+__device__ __forceinline__ void lines_vrr_xy(int lane, const double* Fs, const LinePS& s,
+                                             double* __restrict__ Y) {
+  const int ex = lane;
+  if (ex > L) return;
+  double c[L + 2], p[L + 2];
+#pragma unroll
+  for (int m = 0; m <= L; ++m) {
+    c[m] = Fs[m];
+    p[m] = 0.0;
+  }
+  c[L + 1] = 0.0;
+  p[L + 1] = 0.0;
+#pragma unroll
+  for (int k = 1; k <= L; ++k)
+    if (k <= ex) lines_vstep<L>(c, p, k, s.PAx, s.WPx, s.o2z, s.rz);
+  const int u = L + 1 - ex;
+  const int b0 = lines_tet(L + 1) - lines_tet(u);
+#pragma unroll
+  for (int m = 0; m <= L; ++m)
+    if (m <= L - ex) Y[b0 + m] = c[m];
+#pragma unroll
+  for (int m = 0; m <= L + 1; ++m) p[m] = 0.0;
+#pragma unroll
+  for (int ey = 1; ey <= L; ++ey) {
+    if (ey <= L - ex) {
+      lines_vstep<L>(c, p, ey, s.PAy, s.WPy, s.o2z, s.rz);
+      const int bo = b0 + ey * u - ey * (ey - 1) / 2;
+#pragma unroll
+      for (int m = 0; m <= L - ey; ++m)
+        if (m <= L - ex - ey) Y[bo + m] = c[m];
+    }
+  }
+}
+
+// VRR along z for line (ex, ey) = (ent & 255, ent >> 8); n = L - ex - ey <= NMAX.
+template <int L, int NMAX>
+__device__ __forceinline__ void lines_vrr_z(int ent, const LinePS& s, const double* __restrict__ Y,
+                                            double* __restrict__ W) {
+  if (ent < 0) return;
+  const int ex = ent & 255, ey = ent >> 8;
+  const int n = L - ex - ey;
+  const int b = lines_toff(ex, ey, L);  // same offset in Y and in W block (0, 0)
+  double c[NMAX + 2], p[NMAX + 2];
+#pragma unroll
+  for (int m = 0; m <= NMAX; ++m) {
+    c[m] = (m <= n) ? Y[b + m] : 0.0;
+    p[m] = 0.0;
+  }
+  c[NMAX + 1] = 0.0;
+  p[NMAX + 1] = 0.0;
+  W[b] = c[0];
+#pragma unroll
+  for (int ez = 1; ez <= NMAX; ++ez) {
+    if (ez <= n) {
+      lines_vstep<NMAX>(c, p, ez, s.PAz, s.WPz, s.o2z, s.rz);
+      W[b + ez] = c[0];
+    }
+  }
+}
+
+// Transfer along x for line (ey, ez) = (ent & 255, ent >> 8): cells ex <= n - fx, n = L-ey-ez.
+template <int L, int F, int NMAX>
+__device__ __forceinline__ void lines_etr_x(int ent, const LinePS& s, double* __restrict__ W) {
+  if (ent < 0) return;
+  const int ey = ent & 255, ez = ent >> 8;
+  const int n = L - ey - ez;
+  const int q = ey * (ey - 1) / 2;
+  double r1[NMAX + 2], r0[NMAX + 2];
+#pragma unroll
+  for (int ex = 0; ex <= NMAX; ++ex) {
+    r1[ex] = (ex <= n) ? W[lines_tet(L + 1) - lines_tet(L + 1 - ex) + ey * (L + 1 - ex) - q + ez]
+                       : 0.0;
+    r0[ex] = 0.0;
+  }
+  r1[NMAX + 1] = 0.0;
+  r0[NMAX + 1] = 0.0;
+#pragma unroll
+  for (int fx = 1; fx <= F; ++fx) {
+    if (fx > NMAX) break;
+    const int ext = n - fx;
+    lines_tstep<NMAX>(r1, r0, fx - 1, ext, s.CEx, s.ze, s.o2e, NMAX - fx);
+    const int g = L - fx;
+    const int zb = lines_zb(L, F, fx, 0);
+#pragma unroll
+    for (int ex = 0; ex <= NMAX - fx; ++ex)
+      if (ex <= ext)
+        W[zb + lines_tet(g + 1) - lines_tet(g + 1 - ex) + ey * (g + 1 - ex) - q + ez] = r1[ex];
+  }
+}
+
+// Transfer along y for line (ex, ez) = (ent & 255, ent >> 8) at fx = FX: cells ey <= n - fy,
+// n = min(EMAX + F - FX - ex, L - FX - ex - ez).
+template <int L, int F, int EMAX, int FX, int NMAX>
+__device__ __forceinline__ void lines_etr_y(int ent, const LinePS& s, double* __restrict__ W) {
+  if (ent < 0) return;
+  const int ex = ent & 255, ez = ent >> 8;
+  const int n = min(EMAX + F - FX - ex, L - FX - ex - ez);
+  double r1[NMAX + 2], r0[NMAX + 2];
+  {
+    constexpr int g = L - FX;
+    constexpr int zb = lines_zb(L, F, FX, 0);
+    const int b = zb + lines_tet(g + 1) - lines_tet(g + 1 - ex) + ez;
+    const int u = g + 1 - ex;
+#pragma unroll
+    for (int ey = 0; ey <= NMAX; ++ey) {
+      r1[ey] = (ey <= n) ? W[b + ey * u - ey * (ey - 1) / 2] : 0.0;
+      r0[ey] = 0.0;
+    }
+  }
+  r1[NMAX + 1] = 0.0;
+  r0[NMAX + 1] = 0.0;
+#pragma unroll
+  for (int fy = 1; fy <= F - FX; ++fy) {
+    if (fy > NMAX) break;
+    const int ext = n - fy;
+    lines_tstep<NMAX>(r1, r0, fy - 1, ext, s.CEy, s.ze, s.o2e, NMAX - fy);
+    const int g = L - FX - fy;
+    const int b = lines_zb(L, F, FX, fy) + lines_tet(g + 1) - lines_tet(g + 1 - ex) + ez;
+    const int u = g + 1 - ex;
+#pragma unroll
+    for (int ey = 0; ey <= NMAX - fy; ++ey)
+      if (ey <= ext) W[b + ey * u - ey * (ey - 1) / 2] = r1[ey];
+  }
+}
+
+// Transfer along z for line (ex,ey,fx,fy) = 4-bit fields of ent.x, W offset of its first cell
+// in ent.y; cells ez <= n - fz, n = L - s - t; targets (la <= s+ez <= EMAX, lc <= t+fz <= F)
+// stored (first primitive) or added to ACC[ie * NF + jf].
+template <int L, int F, int LA, int EMAX, int LC, int NF, int NMAX, int FZMAX>
+__device__ __forceinline__ void lines_etr_z(int2 ent, const LinePS& s,
+                                            const double* __restrict__ W, double* __restrict__ ACC,
+                                            bool first) {
+  if (ent.x < 0) return;
+  const int ex = ent.x & 15, ey = (ent.x >> 4) & 15, fx = (ent.x >> 8) & 15, fy = (ent.x >> 12) & 15;
+  const int sl = ex + ey, t = fx + fy;
+  const int n = L - sl - t, fzmax = F - t;
+  double r1[NMAX + 2], r0[NMAX + 2];
+#pragma unroll
+  for (int ez = 0; ez <= NMAX; ++ez) {
+    r1[ez] = (ez <= n) ? W[ent.y + ez] : 0.0;
+    r0[ez] = 0.0;
+  }
+  r1[NMAX + 1] = 0.0;
+  r0[NMAX + 1] = 0.0;
+  const int eb = -lines_tet(LA), fb = -lines_tet(LC);
+#pragma unroll
+  for (int fz = 0; fz <= FZMAX; ++fz) {
+    if (fz > fzmax) break;
+    if (fz >= 1) lines_tstep<NMAX>(r1, r0, fz - 1, n - fz, s.CEz, s.ze, s.o2e, NMAX - fz);
+    const int tf = t + fz;
+    if (tf >= LC) {
+      const int jf = fb + lines_tet(tf) + (fy + fz) * (fy + fz + 1) / 2 + fz;
+#pragma unroll
+      for (int ez = 0; ez <= NMAX - fz; ++ez) {
+        const int se = sl + ez;
+        if (ez <= n - fz && se >= LA && se <= EMAX) {
+          const int ie = eb + lines_tet(se) + (ey + ez) * (ey + ez + 1) / 2 + ez;
+          double* dst = ACC + ie * NF + jf;
+          *dst = first ? r1[ez] : *dst + r1[ez];
+        }
+      }
+    }
+  }
+}
+
+// Register tail of classes whose ket block (NCD) and bra block (NAB) fit a lane: lanes take
+// rows e of ACC and run the ket horizontal recursion and ket transforms in registers (T::ket),
+// writing HF[e][cd]; then lanes take output columns (c, d) and run the bra recursion
+// (T::bra), bra transforms, scaling and the store (mode 0) or the Schwarz maximum (mode 1).
+template <int LA, int LB, int LC, int LD, class T>
+__device__ __forceinline__ void lines_tail(const EriLaunch& a, double* S, const int2 pq,
+                                           const PairDev& P, const PairDev& Q, const int lane,
+                                           int NE, int NF) {
+  constexpr int NCA = ncart(LA), NCB = ncart(LB), NCC = ncart(LC), NCDD = ncart(LD);
+  constexpr int NCD = NCC * NCDD, NAB = NCA * NCB;
+  const double* ACC = S;
+  double* HF = S + NE * NF;
+  const ShellDev& sA = a.shells[P.shA];
+  const ShellDev& sB = a.shells[P.shB];
+  const ShellDev& sC = a.shells[Q.shA];
+  const ShellDev& sD = a.shells[Q.shB];
+  const bool schwarz = a.mode == 1;
+  for (int e = lane; e < NE; e += 32) {
+    double h[NCD];
+    T::ket(ACC + e * NF, Q.ABx, Q.ABy, Q.ABz, h);
+    if (!schwarz) {
+      if (LD >= 2 && sD.sph) sph_axis<LD, NCC, 1>(h);
+      if (LC >= 2 && sC.sph) sph_axis<LC, 1, NCDD>(h);
+    }
+#pragma unroll
+    for (int i = 0; i < NCD; ++i) HF[e * NCD + i] = h[i];
+  }
+  __syncwarp();
+  const int nAi = schwarz ? NCA : internal_count(sA), nBi = schwarz ? NCB : internal_count(sB);
+  const int nCi = schwarz ? NCC : internal_count(sC), nDi = schwarz ? NCDD : internal_count(sD);
+  const int ncol = nCi * nDi;
+  long long bbase, bcols;
+  block_dest(a, P, bbase, bcols);
+  double* __restrict__ dst = a.out + bbase + Q.fo;
+  const long long nBo = sB.nout, nDo = sD.nout;
+  double mx = 0.0;
+  for (int k = lane; k < ncol; k += 32) {
+    const int uc = k / nDi, ud = k - uc * nDi;
+    double o[NAB];
+    T::bra(HF + uc * NCDD + ud, NCD, P.ABx, P.ABy, P.ABz, o);
+    if (schwarz) {
+      const double wcd = gen::cnorm<LC>(uc) * gen::cnorm<LD>(ud);
+#pragma unroll
+      for (int ia = 0; ia < NCA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NCB; ++ib)
+          mx = fmax(mx, fabs(o[ia * NCB + ib]) * (gen::cnorm<LA>(ia) * gen::cnorm<LB>(ib) * wcd));
+      continue;
+    }
+    if (LB >= 2 && sB.sph) sph_axis<LB, NCA, 1>(o);
+    if (LA >= 2 && sA.sph) sph_axis<LA, 1, NCB>(o);
+    const double fcd = sC.scl[uc] * sD.scl[ud];
+    double* __restrict__ col = dst + sC.pos[uc] * nDo + sD.pos[ud];
+#pragma unroll
+    for (int ia = 0; ia < NCA; ++ia) {
+      if (ia >= nAi) break;
+      const double fa = sA.scl[ia] * fcd;
+      const long long ra = (long long)P.fo + sA.pos[ia] * nBo;
+#pragma unroll
+      for (int ib = 0; ib < NCB; ++ib) {
+        if (ib >= nBi) break;
+        col[(ra + sB.pos[ib]) * bcols] = o[ia * NCB + ib] * fa * sB.scl[ib];
+      }
+    }
+  }
+  if (schwarz) {
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) a.qout[pq.x] = sqrt(mx);
+  }
+  __syncwarp();
+}
+
+// The kernel: per quartet, ACC[e][f] over the primitive quartets by C::prim, then the shared
+// tail (HRR, transforms, store / Schwarz / Coulomb epilogue).  Per warp shared memory:
+// ACC | W | Y | Boys values, the tail's buffers overlaying W.
+template <class C, bool COULOMB>
+__global__ void __launch_bounds__(128, 4) eri_lines(const CoopArgs A) {
+  extern __shared__ double smem[];
+  const EriLaunch& a = A.a;
+  const CoopMeta& M = A.m;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  short(*s_ins)[8] = reinterpret_cast<short(*)[8]>(smem);
+  short* s_idx = reinterpret_cast<short*>(smem) + 8 * M.n_ins;
+  const bool staged = A.prog_doubles > 0;
+  if (staged) {
+    const int4* src = reinterpret_cast<const int4*>(&kCoopIns[M.v_ins][0]);
+    int4* dst4 = reinterpret_cast<int4*>(smem);
+    for (int i = threadIdx.x; i < M.n_ins; i += blockDim.x) dst4[i] = src[i];
+    for (int i = threadIdx.x; i < M.n_idx; i += blockDim.x) s_idx[i] = kCoopIdx[M.targets + i];
+    __syncthreads();
+  }
+  const ProgView pv = staged ? ProgView{s_ins, s_idx, M.v_ins, M.targets}
+                             : ProgView{kCoopIns, kCoopIdx, 0, 0};
+  double* S = smem + A.prog_doubles + (size_t)wib * A.smem_per_warp;
+  double* ACC = S;
+  double* W = S + C::NE * C::NF;
+  double* Y = W + C::kW;
+  double* Fs = Y + C::kY;
+  const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + wib; w < count; w += nwarps) {
+    const int2 pq = a.work[a.reverse ? a.work_off + a.nwork - 1 - w : a.work_off + w];
+    const PairDev P = a.pairs[pq.x];
+    const PairDev Q = a.pairs[pq.y];
+    // primitive quartets in one flat loop; the next pair data are loaded one step ahead
+    const int np = P.nprim * Q.nprim;
+    PrimPair bp = a.prims[P.prim_off], kp = a.prims[Q.prim_off];
+    for (int idx = 0; idx < np; ++idx) {
+      PrimPair bpn = bp, kpn = kp;
+      if (idx + 1 < np) {
+        const int ip = (idx + 1) / Q.nprim, jq = idx + 1 - ip * Q.nprim;
+        bpn = a.prims[P.prim_off + ip];
+        kpn = a.prims[Q.prim_off + jq];
+      }
+      const double r = rsqrt(bp.zeta + kp.zeta);
+      const double inv = r * r;
+      const double PQx = bp.Px - kp.Px, PQy = bp.Py - kp.Py, PQz = bp.Pz - kp.Pz;
+      const double rz = kp.zeta * inv;
+      const double T = bp.zeta * rz * fma(PQx, PQx, fma(PQy, PQy, PQz * PQz));
+      LinePS ps;
+      ps.PAx = bp.Xx;
+      ps.PAy = bp.Xy;
+      ps.PAz = bp.Xz;
+      ps.WPx = -rz * PQx;
+      ps.WPy = -rz * PQy;
+      ps.WPz = -rz * PQz;
+      ps.o2z = 0.5 * bp.izeta;
+      ps.rz = rz;
+      ps.ze = bp.zeta * kp.izeta;
+      ps.o2e = 0.5 * kp.izeta;
+      ps.CEx = fma(ps.ze, bp.Xx, kp.Xx);
+      ps.CEy = fma(ps.ze, bp.Xy, kp.Xy);
+      ps.CEz = fma(ps.ze, bp.Xz, kp.Xz);
+      boys_lanes(C::L, lane, T, bp.C * kp.C * r, a.boys_tab, Fs);
+      __syncwarp();
+      C::prim(lane, Fs, ps, W, Y, ACC, idx == 0);
+      __syncwarp();
+      bp = bpn;
+      kp = kpn;
+    }
+    if constexpr (C::kRegTail && !COULOMB) {
+      lines_tail<C::LA, C::LB, C::LC, C::LD, typename C::Tail>(a, S, pq, P, Q, lane, C::NE, C::NF);
+    } else {
+      coop_tail(A, pv, S, pq, P, Q, lane);
+    }
+  }
+}
+
+// Launch of the line kernel of class C (same shared-memory plan as the interpreted kernel,
+// with phase A's W, Y and Boys buffers).
+template <class C>
+int launch_lines_t(const EriLaunch& a, const CoopMeta& m, cudaStream_t st) {
+  CoopArgs A;
+  A.a = a;
+  A.m = m;
+  size_t smem = 0;
+  int wpc = 1;
+  int s = coop_plan(m, (long long)C::kW + C::kY + C::L + 1, A, smem, wpc);
+  if (s) return s;
+  // the Coulomb epilogue (mode 2) is a separate instantiation, so that the store / Schwarz
+  // kernel of a class with the register tail carries no interpreted tail
+  auto kern = a.mode == 2 ? eri_lines<C, true> : eri_lines<C, false>;
+  s = cuda_status(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kCoopMaxSmem), "eri_lines shared memory attribute");
+  if (s) return s;
+  kern<<<coop_grid(a, wpc), 32 * wpc, smem, st>>>(A);
+  return cuda_status(cudaGetLastError(), "eri_lines launch");
+}
+
+}  // namespace gbx
