@@ -36,6 +36,9 @@ sys.path.insert(0, ROOT)
 WORKLOAD = "medium8"
 METRIC = "unique contracted ERIs/s (FP64 full tensor)"
 UNIT = "ERI/s"
+# DRAM bytes of one expand_rows launch on medium8 from an ncu capture (405.0 MB read +
+# 1,603.4 MB written); the algorithmic bytes are 1,913.5 MB
+EXPAND_TRAFFIC_BYTES = 405.030912e6 + 1603.407e6
 
 
 def _peaks():
@@ -396,14 +399,17 @@ def main():
     compute_tf = flops / (ph[1] * 1e-3) / 1e12
     exp_bytes = 8.0 * n ** 4 + compact_bytes  # tensor written + compact store read once
     exp_gbs = exp_bytes / (ph[2] * 1e-3) / 1e9
-    roof_compute = {"kernel": "eri_block_fp64 (all classes)", "bound": "fp64", "achieved": compute_tf,
+    roof_compute = {"kernel": "class kernels (eri_block, eri_split, eri_lines; all class blocks, concurrent)", "bound": "fp64", "achieved": compute_tf,
                     "peak": peak64, "unit": "TFLOP/s", "frac": compute_tf / peak64,
                     "peak_source": "gbx_fp64_peak dependent-FMA probe, measured live",
                     "traffic": None, "ms": ph[1], "algorithmic_flops": flops}
-    roof_expand = {"kernel": "expand_full", "bound": "hbm", "achieved": exp_gbs, "peak": hbm,
+    roof_expand = {"kernel": "expand_rows", "bound": "hbm", "achieved": exp_gbs, "peak": hbm,
                    "unit": "GB/s", "frac": (exp_gbs / hbm) if hbm else None,
                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
-                   "traffic": None, "ms": ph[2], "algorithmic_bytes": exp_bytes}
+                   "traffic": EXPAND_TRAFFIC_BYTES if WORKLOAD == "medium8" else None,
+                   "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                     "expand_rows launch on this workload (--set full capture)",
+                   "ms": ph[2], "algorithmic_bytes": exp_bytes}
     roof = roof_compute if ph[1] >= ph[2] else roof_expand
 
     # end to end through the public API with host buffers
@@ -417,8 +423,20 @@ def main():
         res = er.electron_repulsion_integral(shells, out=pinned)
     e2e_s = (time.perf_counter() - t0) / a.e2e_steps
     assert res.shape == (n, n, n, n)
+    # floor of the host-output path on this machine: one plain device-to-host copy of the
+    # tensor's bytes into the same page-locked buffer
+    src = out.view(-1)[: n ** 4]
+    host = torch.from_numpy(pinned.reshape(-1))
+    host.copy_(src, non_blocking=True)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    host.copy_(src, non_blocking=True)
+    torch.cuda.synchronize()
+    d2h_s = time.perf_counter() - t1
     e2e = {"value": world * n_unique / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": 8 * n ** 4, "ms_per_step": e2e_s * 1e3}
+           "d2h_bytes_per_step": 8 * n ** 4, "ms_per_step": e2e_s * 1e3,
+           "d2h_copy_floor_ms": d2h_s * 1e3,
+           "d2h_copy_gbs": 8 * n ** 4 / d2h_s / 1e9}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",

@@ -26,6 +26,7 @@ the per-class device code.
 """
 from __future__ import annotations
 
+import functools
 import math
 
 
@@ -339,6 +340,8 @@ def emit_sources(outdir, heavy, nfiles=12):
             code, t = emit_class(Schedule(*c), tab_name, len(tab))
             tab += t
             structs.append(code)
+            if split_ok(c):
+                structs.append(emit_split(c))
         out = ["// Generated by gen_lines.py: line-factorised cooperative kernels of heavy classes.",
                f'#include "{prog}"',
                '#include "../lines_kernel.cuh"',
@@ -352,6 +355,8 @@ def emit_sources(outdir, heavy, nfiles=12):
             name = f"launch_lines_{tag}"
             launchers[c] = name
             out.append(f"int {name}(const EriLaunch& a, cudaStream_t st) {{")
+            if split_ok(c):
+                out.append(f"  if (a.mode != 2) return launch_split_t<SplitCls_{tag}>(a, st);")
             out.append(f"  return launch_lines_t<LinesCls_{tag}>(a, kCoopMeta[{j}], st);")
             out.append("}")
         out.append("}  // namespace gbx")
@@ -421,4 +426,108 @@ def emit_tail(cls):
     out += [f"    out[{k}] = {bmap[(a, b)]};" for k, (a, b) in
             enumerate((a, b) for a in G.comps(la) for b in G.comps(lb))]
     out += ["  }", "};"]
+    return "\n".join(out)
+
+
+# ------------------------------------------------------------------- split register kernel
+SPLIT = 4           # warps of a CTA, each computing one part of the targets
+SPLIT_MAX_ACC = 64  # accumulators per thread in a part
+SPLIT_MAX_OPS = 500
+SPLIT_MAX_L = 6
+
+
+def split_parts(cls):
+    """Contiguous ranges of bra rows e (in target order), one per warp."""
+    import gen_eri as G
+    la, lb, lc, ld = cls
+    NE = len(G.comps_range(la, la + lb))
+    return [(r * NE // SPLIT, (r + 1) * NE // SPLIT) for r in range(SPLIT)]
+
+
+def split_ok(cls):
+    """Classes whose parts fit a thread's registers: at most SPLIT_MAX_ACC accumulators and
+    SPLIT_MAX_OPS recursion operations per part (beyond that the parts spill, as measured with
+    ptxas on sm_100a)."""
+    return _split_ok(tuple(cls))
+
+
+@functools.lru_cache(maxsize=None)
+def _split_ok(cls):
+    import gen_eri as G
+    la, lb, lc, ld = cls
+    E = G.comps_range(la, la + lb)
+    F = G.comps_range(lc, lc + ld)
+    parts = split_parts(cls)
+    if not (sum(cls) <= SPLIT_MAX_L and tail_fits(cls) and all(e1 > e0 for e0, e1 in parts)):
+        return False
+    if max(e1 - e0 for e0, e1 in parts) * len(F) > SPLIT_MAX_ACC:
+        return False
+    return max(_part_gen(cls, E[e0:e1], F).op_count() for e0, e1 in parts) <= SPLIT_MAX_OPS
+
+
+def _part_gen(cls, E, F):
+    """Cheapest recursion closure (over the step-direction choices) for targets E x F."""
+    import gen_eri as G
+    la, lb, lc, ld = cls
+    best = None
+    for vp in (G.pick_first, G.pick_last, G.pick_max):
+        for ep in (G.pick_etr_first, G.pick_etr_last, G.pick_etr_max, G.pick_etr_min_e):
+            g = G.PrimGen.__new__(G.PrimGen)
+            g.la, g.lb, g.lc, g.ld = la, lb, lc, ld
+            g.L = sum(cls)
+            g.E, g.F = E, F
+            g.vrr_pick, g.etr_pick = vp, ep
+            g.vrr, g.etr = {}, {}
+            for e in E:
+                for f in F:
+                    g._need_etr(e, f)
+            n = g.op_count()
+            if best is None or n < best[0]:
+                best = (n, g)
+    return best[1]
+
+
+def emit_split(cls):
+    """Struct SplitCls_<tag>: part(r, ...) adds part r's [e0|f0] (rows e0(r)..e1(r)) of one
+    primitive quartet to acc (row-major within the part)."""
+    import gen_eri as G
+    la, lb, lc, ld = cls
+    E = G.comps_range(la, la + lb)
+    F = G.comps_range(lc, lc + ld)
+    parts = split_parts(cls)
+    kacc = max(e1 - e0 for e0, e1 in parts) * len(F)
+    tag = _tag(cls)
+    out = [f"struct SplitCls_{tag} {{",
+           f"  static constexpr int L = {sum(cls)}, NE = {len(E)}, NF = {len(F)}, kAcc = {kacc};",
+           f"  static constexpr int LA = {la}, LB = {lb}, LC = {lc}, LD = {ld};",
+           f"  using Tail = TailCls_{tag};",
+           "  static __device__ __forceinline__ int e0(int r) { return "
+           + " ".join(f"r == {r} ? {e0} :" for r, (e0, _) in enumerate(parts[:-1]))
+           + f" {parts[-1][0]}; }}",
+           "  static __device__ __forceinline__ int ne(int r) { return "
+           + " ".join(f"r == {r} ? {e1 - e0} :" for r, (e0, e1) in enumerate(parts[:-1]))
+           + f" {parts[-1][1] - parts[-1][0]}; }}"]
+    for r, (e0, e1) in enumerate(parts):
+        g = _part_gen(cls, E[e0:e1], F)
+        body = []
+        g.emit(body)
+        out.append(f"  static __device__ __forceinline__ void part{r}(const double* __restrict__ F,")
+        out.append("      double PAx, double PAy, double PAz, double WPx, double WPy, double WPz,")
+        out.append("      double o2z, double rz, double CEx, double CEy, double CEz, double ze, double o2e,")
+        out.append("      double* __restrict__ acc) {")
+        out += ["    " + b.replace("const R ", "const double ").replace("R(", "double(") for b in body]
+        out.append("    (void)PAx; (void)PAy; (void)PAz; (void)WPx; (void)WPy; (void)WPz; (void)o2z;")
+        out.append("    (void)rz; (void)CEx; (void)CEy; (void)CEz; (void)ze; (void)o2e;")
+        out.append("  }")
+    out.append("  static __device__ __forceinline__ void part(int r, const double* F, double PAx,")
+    out.append("      double PAy, double PAz, double WPx, double WPy, double WPz, double o2z, double rz,")
+    out.append("      double CEx, double CEy, double CEz, double ze, double o2e, double* acc) {")
+    out.append("    switch (r) {")
+    for r in range(SPLIT):
+        out.append(f"      case {r}: part{r}(F, PAx, PAy, PAz, WPx, WPy, WPz, o2z, rz, CEx, CEy, CEz, "
+                   "ze, o2e, acc); break;")
+    out.append("      default: break;")
+    out.append("    }")
+    out.append("  }")
+    out.append("};")
     return "\n".join(out)

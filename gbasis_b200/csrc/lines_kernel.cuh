@@ -263,13 +263,11 @@ __device__ __forceinline__ void lines_etr_z(int2 ent, const LinePS& s,
 // writing HF[e][cd]; then lanes take output columns (c, d) and run the bra recursion
 // (T::bra), bra transforms, scaling and the store (mode 0) or the Schwarz maximum (mode 1).
 template <int LA, int LB, int LC, int LD, class T>
-__device__ __forceinline__ void lines_tail(const EriLaunch& a, double* S, const int2 pq,
-                                           const PairDev& P, const PairDev& Q, const int lane,
-                                           int NE, int NF) {
+__device__ __forceinline__ void lines_tail(const EriLaunch& a, const double* ACC, double* HF,
+                                           const int2 pq, const PairDev& P, const PairDev& Q,
+                                           const int lane, int NE, int NF) {
   constexpr int NCA = ncart(LA), NCB = ncart(LB), NCC = ncart(LC), NCDD = ncart(LD);
   constexpr int NCD = NCC * NCDD, NAB = NCA * NCB;
-  const double* ACC = S;
-  double* HF = S + NE * NF;
   const ShellDev& sA = a.shells[P.shA];
   const ShellDev& sB = a.shells[P.shB];
   const ShellDev& sC = a.shells[Q.shA];
@@ -400,7 +398,8 @@ __global__ void __launch_bounds__(128, 4) eri_lines(const CoopArgs A) {
       kp = kpn;
     }
     if constexpr (C::kRegTail && !COULOMB) {
-      lines_tail<C::LA, C::LB, C::LC, C::LD, typename C::Tail>(a, S, pq, P, Q, lane, C::NE, C::NF);
+      lines_tail<C::LA, C::LB, C::LC, C::LD, typename C::Tail>(a, S, S + C::NE * C::NF, pq, P, Q,
+                                                               lane, C::NE, C::NF);
     } else {
       coop_tail(A, pv, S, pq, P, Q, lane);
     }
@@ -426,6 +425,90 @@ int launch_lines_t(const EriLaunch& a, const CoopMeta& m, cudaStream_t st) {
   if (s) return s;
   kern<<<coop_grid(a, wpc), 32 * wpc, smem, st>>>(A);
   return cuda_status(cudaGetLastError(), "eri_lines launch");
+}
+
+// Split register kernel for heavy classes of moderate size: a CTA of SPLIT = 4 warps takes 32
+// quartets at a time, thread t of warp r computing part r (a contiguous range of bra rows e)
+// of quartet t's contracted [e0|f0] in registers (generated straight-line recursions, as in
+// the light classes' kernel); the parts meet in shared memory ACC[32][NE*NF] and each warp then
+// runs the register tail for 8 of the quartets.  Store (mode 0) and Schwarz (mode 1) only.
+template <class C>
+__global__ void __launch_bounds__(128) eri_split(const EriLaunch a) {
+  __shared__ double s_tab[kBoysNGrid * kBoysTaylor];
+  __shared__ double s_exp[kBoysNGrid];
+  extern __shared__ double dyn[];
+  constexpr int L = C::L;
+  constexpr int NENF = C::NE * C::NF;
+  constexpr int NCD = ncart(C::LC) * ncart(C::LD);
+  stage_boys<L>(a.boys_tab, s_tab, s_exp);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* ACC = dyn;
+  double* HF = dyn + 32 * NENF + warp * C::NE * NCD;
+  const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
+  for (long long base = (long long)blockIdx.x * 32; base < count; base += (long long)gridDim.x * 32) {
+    const long long w = base + lane;
+    if (w < count) {
+      const int2 pq = a.work[a.reverse ? a.work_off + a.nwork - 1 - w : a.work_off + w];
+      const PairDev P = a.pairs[pq.x];
+      const PairDev Q = a.pairs[pq.y];
+      double acc[C::kAcc];
+#pragma unroll
+      for (int i = 0; i < C::kAcc; ++i) acc[i] = 0.0;
+      for (int ip = 0; ip < P.nprim; ++ip) {
+        const PrimPair bp = a.prims[P.prim_off + ip];
+        const double o2z = 0.5 * bp.izeta;
+        for (int jq = 0; jq < Q.nprim; ++jq) {
+          const PrimPair kp = a.prims[Q.prim_off + jq];
+          const double r = rsqrt(bp.zeta + kp.zeta);
+          const double inv = r * r;
+          const double PQx = bp.Px - kp.Px, PQy = bp.Py - kp.Py, PQz = bp.Pz - kp.Pz;
+          const double rz = kp.zeta * inv;
+          const double T = bp.zeta * rz * fma(PQx, PQx, fma(PQy, PQy, PQz * PQz));
+          double F[L + 1];
+          boys_eval<L>(T, s_tab, s_exp, F);
+          const double pref = bp.C * kp.C * r;
+#pragma unroll
+          for (int m = 0; m <= L; ++m) F[m] *= pref;
+          const double ze = bp.zeta * kp.izeta;
+          C::part(warp, F, bp.Xx, bp.Xy, bp.Xz, -rz * PQx, -rz * PQy, -rz * PQz, o2z, rz,
+                  fma(ze, bp.Xx, kp.Xx), fma(ze, bp.Xy, kp.Xy), fma(ze, bp.Xz, kp.Xz), ze,
+                  0.5 * kp.izeta, acc);
+        }
+      }
+      const int nv = C::ne(warp) * C::NF;
+      double* dst = ACC + lane * NENF + C::e0(warp) * C::NF;
+#pragma unroll
+      for (int i = 0; i < C::kAcc; ++i)
+        if (i < nv) dst[i] = acc[i];
+    }
+    __syncthreads();
+    for (int q = warp; q < 32; q += 4) {
+      const long long wq = base + q;
+      if (wq >= count) break;
+      const int2 pq = a.work[a.reverse ? a.work_off + a.nwork - 1 - wq : a.work_off + wq];
+      const PairDev P = a.pairs[pq.x];
+      const PairDev Q = a.pairs[pq.y];
+      lines_tail<C::LA, C::LB, C::LC, C::LD, typename C::Tail>(a, ACC + q * NENF, HF, pq, P, Q,
+                                                               lane, C::NE, C::NF);
+    }
+    __syncthreads();
+  }
+}
+
+template <class C>
+int launch_split_t(const EriLaunch& a, cudaStream_t st) {
+  constexpr int NCD = ncart(C::LC) * ncart(C::LD);
+  const size_t dyn = (size_t)(32 * C::NE * C::NF + 4 * C::NE * NCD) * sizeof(double);
+  int s = cuda_status(cudaFuncSetAttribute(eri_split<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)dyn), "eri_split shared memory attribute");
+  if (s) return s;
+  int dev = 0, nsm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = (int)std::max<long long>(1, std::min<long long>((a.nwork + 31) / 32, (long long)nsm * 4));
+  eri_split<C><<<grid, 128, dyn, st>>>(a);
+  return cuda_status(cudaGetLastError(), "eri_split launch");
 }
 
 }  // namespace gbx

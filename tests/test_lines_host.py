@@ -278,3 +278,40 @@ def test_every_heavy_class_schedules_and_fits():
         assert per_warp < 200 * 1024, c
         code, tab = gen_lines.emit_class(S, "kLinesTab", 0)
         assert all(-1 <= v < (1 << 16) for v in tab)
+
+
+SPLIT = [c for c in HEAVY if gen_lines.split_ok(c)]
+
+
+@pytest.mark.parametrize("cls", SPLIT)
+def test_split_parts_cover_targets(cls):
+    """The split kernel's per-warp parts (generated straight-line recursions, executed here
+    as Python) reassemble the full [e0|f0] at the rows e0(r).. of each part."""
+    from oracle import eri_oracle as orc
+    rng = np.random.default_rng(3 + sum(cls))
+    L = sum(cls)
+    Fs = [float(orc.boys(m, 0.6)) for m in range(L + 1)]
+    s = {"PA": rng.uniform(-0.4, 0.4, 3), "WP": rng.uniform(-0.4, 0.4, 3),
+         "CE": rng.uniform(-0.4, 0.4, 3), "o2z": 0.35, "rz": 0.45, "ze": 0.8, "o2e": 0.3}
+    code = gen_lines.emit_split(cls)
+    la, lb, lc, ld = cls
+    E = gen_eri.comps_range(la, la + lb)
+    F = gen_eri.comps_range(lc, lc + ld)
+    parts = gen_lines.split_parts(cls)
+    got = np.full(len(E) * len(F), np.nan)
+    bodies = re.split(r"static __device__ __forceinline__ void part\d\(", code)[1:1 + len(parts)]
+    for (e0, e1), body in zip(parts, bodies):
+        body = body.split("{", 1)[1].split("\n  }\n", 1)[0]
+        lines = [ln.strip().rstrip(";") for ln in body.split("\n")]
+        lines = [re.sub(r"^const double ", "", ln) for ln in lines
+                 if ln and not ln.startswith("(void)") and ln != "}"]
+        acc = [0.0] * ((e1 - e0) * len(F))
+        env = dict(fma=lambda x, y, w: x * y + w, double=float, F=Fs, acc=acc,
+                   PAx=s["PA"][0], PAy=s["PA"][1], PAz=s["PA"][2], WPx=s["WP"][0], WPy=s["WP"][1],
+                   WPz=s["WP"][2], o2z=s["o2z"], rz=s["rz"], CEx=s["CE"][0], CEy=s["CE"][1],
+                   CEz=s["CE"][2], ze=s["ze"], o2e=s["o2e"])
+        exec("\n".join(lines), env)
+        got[e0 * len(F):e1 * len(F)] = acc
+    Ed = direct(cls, s, Fs)
+    ref = np.array([Ed(e, f) for e in E for f in F])
+    np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())
