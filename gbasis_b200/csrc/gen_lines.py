@@ -430,24 +430,25 @@ def emit_tail(cls):
 
 
 # ------------------------------------------------------------------- split register kernel
-SPLIT = 4           # warps of a CTA, each computing one part of the targets
+SPLITS = (4, 8)     # warps of a CTA, each computing one part of the targets
 SPLIT_MAX_ACC = 64  # accumulators per thread in a part
 SPLIT_MAX_OPS = 500
-SPLIT_MAX_L = 6
+SPLIT_MAX_L = 7
 
 
-def split_parts(cls):
+def split_parts(cls, S):
     """Contiguous ranges of bra rows e (in target order), one per warp."""
     import gen_eri as G
     la, lb, lc, ld = cls
     NE = len(G.comps_range(la, la + lb))
-    return [(r * NE // SPLIT, (r + 1) * NE // SPLIT) for r in range(SPLIT)]
+    return [(r * NE // S, (r + 1) * NE // S) for r in range(S)]
 
 
 def split_ok(cls):
-    """Classes whose parts fit a thread's registers: at most SPLIT_MAX_ACC accumulators and
-    SPLIT_MAX_OPS recursion operations per part (beyond that the parts spill, as measured with
-    ptxas on sm_100a)."""
+    """Number of parts (warps) of the split kernel for the class, or 0: the smallest S whose
+    parts fit a thread's registers (at most SPLIT_MAX_ACC accumulators and SPLIT_MAX_OPS
+    recursion operations per part, or 620 operations with at most 40 accumulators; beyond that
+    the parts spill, as measured with ptxas on sm_100a)."""
     return _split_ok(tuple(cls))
 
 
@@ -457,12 +458,19 @@ def _split_ok(cls):
     la, lb, lc, ld = cls
     E = G.comps_range(la, la + lb)
     F = G.comps_range(lc, lc + ld)
-    parts = split_parts(cls)
-    if not (sum(cls) <= SPLIT_MAX_L and tail_fits(cls) and all(e1 > e0 for e0, e1 in parts)):
-        return False
-    if max(e1 - e0 for e0, e1 in parts) * len(F) > SPLIT_MAX_ACC:
-        return False
-    return max(_part_gen(cls, E[e0:e1], F).op_count() for e0, e1 in parts) <= SPLIT_MAX_OPS
+    if not (sum(cls) <= SPLIT_MAX_L and tail_fits(cls)):
+        return 0
+    for S in SPLITS:
+        parts = split_parts(cls, S)
+        if not all(e1 > e0 for e0, e1 in parts):
+            continue
+        acc = max(e1 - e0 for e0, e1 in parts) * len(F)
+        if acc > SPLIT_MAX_ACC:
+            continue
+        ops = max(_part_gen(cls, E[e0:e1], F).op_count() for e0, e1 in parts)
+        if ops <= SPLIT_MAX_OPS or (acc <= 40 and ops <= 620):
+            return S
+    return 0
 
 
 def _part_gen(cls, E, F):
@@ -494,11 +502,13 @@ def emit_split(cls):
     la, lb, lc, ld = cls
     E = G.comps_range(la, la + lb)
     F = G.comps_range(lc, lc + ld)
-    parts = split_parts(cls)
+    S = split_ok(cls)
+    parts = split_parts(cls, S)
     kacc = max(e1 - e0 for e0, e1 in parts) * len(F)
     tag = _tag(cls)
     out = [f"struct SplitCls_{tag} {{",
-           f"  static constexpr int L = {sum(cls)}, NE = {len(E)}, NF = {len(F)}, kAcc = {kacc};",
+           f"  static constexpr int L = {sum(cls)}, NE = {len(E)}, NF = {len(F)}, kAcc = {kacc}, "
+           f"kS = {S};",
            f"  static constexpr int LA = {la}, LB = {lb}, LC = {lc}, LD = {ld};",
            f"  using Tail = TailCls_{tag};",
            "  static __device__ __forceinline__ int e0(int r) { return "
@@ -523,7 +533,7 @@ def emit_split(cls):
     out.append("      double PAy, double PAz, double WPx, double WPy, double WPz, double o2z, double rz,")
     out.append("      double CEx, double CEy, double CEz, double ze, double o2e, double* acc) {")
     out.append("    switch (r) {")
-    for r in range(SPLIT):
+    for r in range(S):
         out.append(f"      case {r}: part{r}(F, PAx, PAy, PAz, WPx, WPy, WPz, o2z, rz, CEx, CEy, CEz, "
                    "ze, o2e, acc); break;")
     out.append("      default: break;")

@@ -427,13 +427,14 @@ int launch_lines_t(const EriLaunch& a, const CoopMeta& m, cudaStream_t st) {
   return cuda_status(cudaGetLastError(), "eri_lines launch");
 }
 
-// Split register kernel for heavy classes of moderate size: a CTA of SPLIT = 4 warps takes 32
-// quartets at a time, thread t of warp r computing part r (a contiguous range of bra rows e)
-// of quartet t's contracted [e0|f0] in registers (generated straight-line recursions, as in
-// the light classes' kernel); the parts meet in shared memory ACC[32][NE*NF] and each warp then
-// runs the register tail for 8 of the quartets.  Store (mode 0) and Schwarz (mode 1) only.
+// Split register kernel for heavy classes of moderate size: a CTA of S = C::kS warps (4 or 8)
+// takes 32 quartets at a time, thread t of warp r computing part r (a contiguous range of bra
+// rows e) of quartet t's contracted [e0|f0] in registers (generated straight-line recursions,
+// as in the light classes' kernel); the parts meet in shared memory ACC[32][NE*NF] and each
+// warp then runs the register tail for 32 / S of the quartets.  Store (mode 0) and Schwarz
+// (mode 1) only.
 template <class C>
-__global__ void __launch_bounds__(128) eri_split(const EriLaunch a) {
+__global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
   __shared__ double s_tab[kBoysNGrid * kBoysTaylor];
   __shared__ double s_exp[kBoysNGrid];
   extern __shared__ double dyn[];
@@ -483,7 +484,7 @@ __global__ void __launch_bounds__(128) eri_split(const EriLaunch a) {
         if (i < nv) dst[i] = acc[i];
     }
     __syncthreads();
-    for (int q = warp; q < 32; q += 4) {
+    for (int q = warp; q < 32; q += C::kS) {
       const long long wq = base + q;
       if (wq >= count) break;
       const int2 pq = a.work[a.reverse ? a.work_off + a.nwork - 1 - wq : a.work_off + wq];
@@ -499,15 +500,15 @@ __global__ void __launch_bounds__(128) eri_split(const EriLaunch a) {
 template <class C>
 int launch_split_t(const EriLaunch& a, cudaStream_t st) {
   constexpr int NCD = ncart(C::LC) * ncart(C::LD);
-  const size_t dyn = (size_t)(32 * C::NE * C::NF + 4 * C::NE * NCD) * sizeof(double);
+  const size_t dyn = (size_t)(32 * C::NE * C::NF + C::kS * C::NE * NCD) * sizeof(double);
   int s = cuda_status(cudaFuncSetAttribute(eri_split<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)dyn), "eri_split shared memory attribute");
   if (s) return s;
   int dev = 0, nsm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = (int)std::max<long long>(1, std::min<long long>((a.nwork + 31) / 32, (long long)nsm * 4));
-  eri_split<C><<<grid, 128, dyn, st>>>(a);
+  const int grid = (int)std::max<long long>(1, std::min<long long>((a.nwork + 31) / 32, (long long)nsm * (32 / C::kS)));
+  eri_split<C><<<grid, 32 * C::kS, dyn, st>>>(a);
   return cuda_status(cudaGetLastError(), "eri_split launch");
 }
 

@@ -297,7 +297,7 @@ def test_split_parts_cover_targets(cls):
     la, lb, lc, ld = cls
     E = gen_eri.comps_range(la, la + lb)
     F = gen_eri.comps_range(lc, lc + ld)
-    parts = gen_lines.split_parts(cls)
+    parts = gen_lines.split_parts(cls, gen_lines.split_ok(cls))
     got = np.full(len(E) * len(F), np.nan)
     bodies = re.split(r"static __device__ __forceinline__ void part\d\(", code)[1:1 + len(parts)]
     for (e0, e1), body in zip(parts, bodies):
