@@ -31,6 +31,8 @@ EXPORTED_SYMBOLS = (
     "gbx_eri_full_mixed", "gbx_eri_unique",
     "gbx_batch_create", "gbx_batch_destroy", "gbx_batch_info", "gbx_batch_run",
     "gbx_batch_set_graph", "gbx_unique_values", "gbx_compact_view",
+    "gbx_batch_num_types", "gbx_batch_type_info", "gbx_batch_set_team", "gbx_batch_set_profiling",
+    "gbx_batch_type_times",
 )
 
 
@@ -93,6 +95,12 @@ def lib():
             "gbx_batch_set_graph": [_P, _I],
             "gbx_unique_values": [_P, _I64, _P, _P, _P],
             "gbx_compact_view": [_P, ctypes.POINTER(_P), ctypes.POINTER(_I64)],
+            "gbx_batch_num_types": [_P, ctypes.POINTER(_I)],
+            "gbx_batch_type_info": [_P, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(_D),
+                                    ctypes.POINTER(_I64)],
+            "gbx_batch_set_team": [_P, _I, _I],
+            "gbx_batch_set_profiling": [_P, _I],
+            "gbx_batch_type_times": [_P, _P, _I],
         }
         for name, args in sig.items():
             f = getattr(L, name)

@@ -4,12 +4,14 @@ A class block holds every quartet of one (bra pair class, ket pair class); its r
 kernel splits each quartet's primitive loop over `team` lanes (1..32) and sums the partial
 [e0|f0] with warp shuffles.  Few primitives favour small teams (no reduction, more
 quartets in flight); heavily contracted quartets favour large ones (parallel primitive
-loop, balanced warps).  The tuner times every block for each candidate on the device (CUDA
-events on the launching stream, one full call per candidate) and keeps the fastest.
+loop, balanced warps).  The tuner times every register-kernel block for each candidate on
+the device (CUDA events on the launching stream, one unique-integral call per candidate, the
+blocks run one after another) and keeps the fastest; ``EriBatch.autotune`` does the same for
+the block types of a batch.
 
 Choices are stored in a JSON cache keyed by class and log2 of the block's mean primitive
-quartets per shell quartet, so a new basis of similar shape starts tuned
-(``DeviceBasis`` applies the cache on creation).
+quartets per shell quartet, so a new basis or batch of similar shape starts tuned
+(``DeviceBasis`` and ``EriBatch`` apply the cache on creation).
 """
 from __future__ import annotations
 
@@ -24,6 +26,18 @@ from . import _engine
 __all__ = ["autotune", "apply_cache", "cache_path", "TEAMS"]
 
 TEAMS = (1, 2, 4, 8, 16, 32)
+
+
+def light_class(cls4):
+    """Classes run by the register kernel (the only ones whose team matters): the [e0|f0]
+    accumulators and the (ab|cd) block of one quartet fit one thread (170 doubles, the limit
+    the kernel generator uses)."""
+    def nc(l):
+        return (l + 1) * (l + 2) // 2
+    la, lb, lc, ld = cls4
+    ne = sum(nc(e) for e in range(la, la + lb + 1))
+    nf = sum(nc(f) for f in range(lc, lc + ld + 1))
+    return ne * nf + nc(la) * nc(lb) * nc(lc) * nc(ld) <= 170
 
 
 def cache_path():
@@ -57,23 +71,23 @@ def apply_cache(db, table=None):
 
 def autotune(shells, coord_types=None, reps=3, teams=TEAMS, save=True, device=None):
     """Tune the teams of ``shells``'s class blocks; returns {key: team} and the timings."""
-    import torch
+    # the unique-integral call runs the same class kernels without the N^4 tensor
     db = _engine.DeviceBasis(shells, coord_types, device=device)
-    n = db.nbf
-    out = torch.empty(n ** 4, dtype=torch.float64, device=torch.device("cuda", db.device))
     db.set_profiling(2)
     blocks = db.blocks()
+    light = [k for k, (cls4, _, _, _) in enumerate(blocks) if light_class(cls4)]
     times = np.full((len(teams), len(blocks)), np.inf)
-    db.full_device(out.data_ptr())
+    db.unique()
     for ti, t in enumerate(teams):
-        for k in range(len(blocks)):
+        for k in light:
             db.set_team(k, t)
         for _ in range(reps):
-            db.full_device(out.data_ptr())
+            db.unique()
             times[ti] = np.minimum(times[ti], db.block_times())
     table = _load()
     chosen = {}
-    for k, (cls4, _, avg, _) in enumerate(blocks):
+    for k in light:
+        cls4, _, avg, _ = blocks[k]
         best = teams[int(np.argmin(times[:, k]))]
         db.set_team(k, best)
         chosen[_key(cls4, avg)] = best

@@ -45,6 +45,73 @@ class EriBatch:
         self.n_quartets, self.compact_bytes = int(q.value), int(cb.value)
         if not graph:
             _engine.check(L.gbx_batch_set_graph(h, 0))
+        self.apply_tuning()
+
+    # ------------------------------------------------------------------ autotuner
+    def types(self):
+        """[(class (la, lb, lc, ld), team, mean primitive quartets, quartets)] per block type."""
+        L = _engine.lib()
+        n = ctypes.c_int()
+        _engine.check(L.gbx_batch_num_types(self.handle, ctypes.byref(n)))
+        out = []
+        for k in range(n.value):
+            c4 = np.zeros(4, dtype=np.int32)
+            t, ap, nq = ctypes.c_int(), ctypes.c_double(), ctypes.c_int64()
+            _engine.check(L.gbx_batch_type_info(self.handle, k, _engine._ptr(c4), ctypes.byref(t),
+                                                ctypes.byref(ap), ctypes.byref(nq)))
+            out.append((tuple(int(v) for v in c4), t.value, ap.value, nq.value))
+        return out
+
+    def set_team(self, k, team):
+        _engine.check(_engine.lib().gbx_batch_set_team(self.handle, int(k), int(team)),
+                      "gbx_batch_set_team")
+
+    def apply_tuning(self, table=None):
+        """Teams from the tuning cache (keyed by class and primitive bucket, shared with the
+        single-basis tuner); returns how many types changed."""
+        from .autotune import _key, _load
+        table = _load() if table is None else table
+        n = 0
+        for k, (cls4, team, avg, _) in enumerate(self.types()):
+            t = table.get(_key(cls4, avg))
+            if t and t != team:
+                self.set_team(k, int(t))
+                n += 1
+        return n
+
+    def autotune(self, outs, teams=None, reps=2, save=True, stream=None):
+        """Time every register-kernel block type with each team (types run one after another,
+        CUDA events per type), keep the fastest, store the choices in the tuning cache."""
+        import json
+        from .autotune import TEAMS, _key, _load, cache_path, light_class
+        teams = TEAMS if teams is None else teams
+        L = _engine.lib()
+        types = self.types()
+        light = [k for k, (c4, _, _, _) in enumerate(types) if light_class(c4)]
+        times = np.full((len(teams), len(types)), np.inf)
+        _engine.check(L.gbx_batch_set_profiling(self.handle, 1))
+        try:
+            for ti, t in enumerate(teams):
+                for k in light:
+                    self.set_team(k, t)
+                for _ in range(reps):
+                    self.run(outs, stream=stream)
+                    ms = np.zeros(len(types))
+                    _engine.check(L.gbx_batch_type_times(self.handle, _engine._ptr(ms), len(ms)))
+                    times[ti] = np.minimum(times[ti], ms)
+        finally:
+            _engine.check(L.gbx_batch_set_profiling(self.handle, 0))
+        chosen = {}
+        for k in light:
+            best = teams[int(np.argmin(times[:, k]))]
+            self.set_team(k, best)
+            chosen[_key(types[k][0], types[k][2])] = best
+        if save:
+            table = _load()
+            table.update(chosen)
+            with open(cache_path(), "w") as f:
+                json.dump(table, f, indent=1, sort_keys=True)
+        return chosen, times
 
     def run(self, outs, notation="chemist", stream=None):
         """Write molecule m's (N_m,)*4 float64 tensor to device buffer ``outs[m]`` (torch

@@ -68,6 +68,9 @@ struct Batch {
   cudaGraphExec_t graph_exec = nullptr;
   bool use_graph = true;
   bool exp_dirty = true;
+  // per-type timing (autotuner): types run one after another on the exec stream, eagerly
+  bool profile = false;
+  std::vector<cudaEvent_t> type_ev;
   std::vector<void*> allocs;
 
   int alloc(void** p, size_t bytes, const char* what) {
@@ -92,6 +95,7 @@ struct Batch {
     for (void* p : allocs) cudaFree(p);
     for (cudaStream_t s : aux) cudaStreamDestroy(s);
     for (cudaEvent_t e : join) cudaEventDestroy(e);
+    for (cudaEvent_t e : type_ev) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
@@ -296,6 +300,7 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st) {
   for (cudaStream_t a : Bt.aux) GBX_CUDA(cudaStreamWaitEvent(a, Bt.fork, 0), "fork wait");
   for (size_t i = 0; i < Bt.order.size(); ++i) {
     const BatchType& T = Bt.types[Bt.order[i]];
+    if (Bt.profile) GBX_CUDA(cudaEventRecord(Bt.type_ev[i], st), "type event");
     EriLaunch a;
     memset(&a, 0, sizeof(a));
     a.pairs = Bt.d_pairs;
@@ -313,9 +318,11 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st) {
     const int grid = (int)std::max<long long>(
         1, std::min<long long>((T.n * T.team + 127) / 128, (long long)nsm * 8));
     int s = launch_class(kPairClassL[T.cb][0], kPairClassL[T.cb][1], kPairClassL[T.ck][0],
-                         kPairClassL[T.ck][1], a, grid, Bt.aux[i % Bt.aux.size()]);
+                         kPairClassL[T.ck][1], a, grid,
+                         Bt.profile ? st : Bt.aux[i % Bt.aux.size()]);
     if (s) return s;
   }
+  if (Bt.profile) GBX_CUDA(cudaEventRecord(Bt.type_ev[Bt.order.size()], st), "type event");
   for (size_t j = 0; j < Bt.aux.size(); ++j) {
     GBX_CUDA(cudaEventRecord(Bt.join[j], Bt.aux[j]), "join");
     GBX_CUDA(cudaStreamWaitEvent(st, Bt.join[j], 0), "join wait");
@@ -342,7 +349,8 @@ static int run_batch(Batch& Bt, int notation, double* const* outs, cudaStream_t 
     GBX_CUDA(cudaStreamSynchronize(Bt.exec), "upload batch descriptors");
     Bt.exp_dirty = false;
   }
-  if (Bt.use_graph && !Bt.graph_exec) {
+  const bool graph = Bt.use_graph && !Bt.profile;
+  if (graph && !Bt.graph_exec) {
     GBX_CUDA(cudaStreamBeginCapture(Bt.exec, cudaStreamCaptureModeRelaxed), "begin capture");
     const int s = enqueue_batch(Bt, Bt.exec);
     cudaGraph_t g = nullptr;
@@ -355,7 +363,7 @@ static int run_batch(Batch& Bt, int notation, double* const* outs, cudaStream_t 
     Bt.graph = g;
     GBX_CUDA(cudaGraphInstantiate(&Bt.graph_exec, g, 0), "instantiate batch graph");
   }
-  if (Bt.use_graph) {
+  if (graph) {
     GBX_CUDA(cudaGraphLaunch(Bt.graph_exec, Bt.exec), "launch batch graph");
   } else {
     const int s = enqueue_batch(Bt, Bt.exec);
@@ -414,6 +422,78 @@ int gbx_batch_info(const gbx_batch* b, int64_t* nbf, int64_t* n_quartets, int64_
 int gbx_batch_set_graph(gbx_batch* b, int on) {
   if (!b) return set_error(GBX_ERR_INVALID, "gbx_batch_set_graph: null batch");
   b->impl->use_graph = on != 0;
+  return GBX_OK;
+}
+
+// Drops the captured graph so that the next run captures the current launch parameters.
+static void batch_drop_graph(Batch& B) {
+  if (B.graph_exec) cudaGraphExecDestroy(B.graph_exec);
+  if (B.graph) cudaGraphDestroy(B.graph);
+  B.graph_exec = nullptr;
+  B.graph = nullptr;
+}
+
+int gbx_batch_num_types(const gbx_batch* b, int* n) {
+  if (!b || !n) return set_error(GBX_ERR_INVALID, "gbx_batch_num_types: null argument");
+  *n = (int)b->impl->types.size();
+  return GBX_OK;
+}
+
+int gbx_batch_type_info(const gbx_batch* b, int k, int* cls4, int* team, double* avg_prims,
+                        int64_t* n_quartets) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_batch_type_info: null batch");
+  const Batch& B = *b->impl;
+  if (k < 0 || k >= (int)B.types.size()) return set_error(GBX_ERR_INVALID, "type %d out of range", k);
+  const BatchType& T = B.types[k];
+  if (cls4) {
+    cls4[0] = kPairClassL[T.cb][0];
+    cls4[1] = kPairClassL[T.cb][1];
+    cls4[2] = kPairClassL[T.ck][0];
+    cls4[3] = kPairClassL[T.ck][1];
+  }
+  if (team) *team = T.team;
+  if (avg_prims) *avg_prims = T.avg_prims;
+  if (n_quartets) *n_quartets = T.n;
+  return GBX_OK;
+}
+
+int gbx_batch_set_team(gbx_batch* b, int k, int team) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_batch_set_team: null batch");
+  Batch& B = *b->impl;
+  if (k < 0 || k >= (int)B.types.size()) return set_error(GBX_ERR_INVALID, "type %d out of range", k);
+  if (team < 1 || team > 32 || (team & (team - 1)))
+    return set_error(GBX_ERR_INVALID, "team must be a power of two in [1, 32]");
+  if (B.types[k].team != team) {
+    B.types[k].team = team;
+    batch_drop_graph(B);
+  }
+  return GBX_OK;
+}
+
+int gbx_batch_set_profiling(gbx_batch* b, int on) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_batch_set_profiling: null batch");
+  Batch& B = *b->impl;
+  DeviceGuardLite g(B.device);
+  if (on && B.type_ev.empty()) {
+    B.type_ev.resize(B.types.size() + 1);
+    for (cudaEvent_t& e : B.type_ev) GBX_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+  }
+  B.profile = on != 0;
+  return GBX_OK;
+}
+
+int gbx_batch_type_times(gbx_batch* b, double* ms, int n) {
+  if (!b || !ms) return set_error(GBX_ERR_INVALID, "gbx_batch_type_times: null argument");
+  Batch& B = *b->impl;
+  if (!B.profile) return set_error(GBX_ERR_INVALID, "profiling is off");
+  if (n < (int)B.types.size()) return set_error(GBX_ERR_INVALID, "ms holds %d < %d types", n, (int)B.types.size());
+  DeviceGuardLite g(B.device);
+  GBX_CUDA(cudaEventSynchronize(B.type_ev[B.order.size()]), "type events");
+  for (size_t i = 0; i < B.order.size(); ++i) {
+    float t = 0.f;
+    GBX_CUDA(cudaEventElapsedTime(&t, B.type_ev[i], B.type_ev[i + 1]), "type elapsed time");
+    ms[B.order[i]] = t;
+  }
   return GBX_OK;
 }
 

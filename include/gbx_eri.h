@@ -161,6 +161,16 @@ int gbx_batch_info(const gbx_batch* b, int64_t* nbf, int64_t* n_quartets,
 int gbx_batch_run(gbx_batch* b, int notation, double* const* outs, void* stream);
 /* 1 (default): replay a captured CUDA graph; 0: launch eagerly every run. */
 int gbx_batch_set_graph(gbx_batch* b, int on);
+/* Block types of a batch (one class kernel launch each) and their team of lanes per quartet
+ * (register kernel; the autotuner's knob).  Setting a team drops the captured graph.  With
+ * profiling on, runs launch the types one after another (no graph) and gbx_batch_type_times
+ * returns each type's kernel time (ms) of the last run. */
+int gbx_batch_num_types(const gbx_batch* b, int* n);
+int gbx_batch_type_info(const gbx_batch* b, int k, int* cls4, int* team, double* avg_prims,
+                        int64_t* n_quartets);
+int gbx_batch_set_team(gbx_batch* b, int k, int team);
+int gbx_batch_set_profiling(gbx_batch* b, int on);
+int gbx_batch_type_times(gbx_batch* b, double* ms, int n);
 
 /* Coulomb matrix J[a,b] = sum_cd (ab|cd) D[c,d] from the screened unique quartets
  * (full tensor never stored).  D, J: device N x N row-major (D symmetric). */

@@ -87,3 +87,24 @@ def test_batch_rejects_bad_outputs():
     with pytest.raises(ValueError):
         b.run(outs, "neither")
     b.close()
+
+
+def test_batch_autotuner_keeps_values():
+    """Per-type timing with each team, the fastest kept; values unchanged up to the order of
+    the primitive sums."""
+    import torch
+    mols = [batch_molecule(m) for m in range(100, 116)]
+    b = EriBatch(mols)
+    outs = [torch.empty((n,) * 4, dtype=torch.float64, device="cuda") for n in b.nbf]
+    b.run(outs)
+    torch.cuda.synchronize()
+    ref = [o.clone() for o in outs]
+    chosen, times = b.autotune(outs, teams=(1, 4, 32), reps=1, save=False)
+    assert chosen and np.isfinite(times).any()
+    for k, (c4, team, avg, nq) in enumerate(b.types()):
+        assert team in (1, 2, 4, 8, 16, 32)
+    b.run(outs)
+    torch.cuda.synchronize()
+    for o, r in zip(outs, ref):
+        np.testing.assert_allclose(o.cpu().numpy(), r.cpu().numpy(), rtol=0, atol=1e-13)
+    b.close()
