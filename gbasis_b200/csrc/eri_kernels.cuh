@@ -21,7 +21,7 @@ __device__ __forceinline__ constexpr double inv_odd(int m) { return 1.0 / (2 * m
 
 // Boys function F_0..F_L(T).  T < 40: Taylor expansion of F_L around the nearest grid point
 // T_n = n/10 (8 terms, |T - T_n| <= 0.05, remainder < 1e-15 relative) from the staged table
-// g[n][k] = F_{L+k}(T_n)/k!, e^{-T} = e^{-T_n} e^{T_n - T} by the same Taylor series, then
+// g[k][n] = F_{L+k}(T_n)/k!, e^{-T} = e^{-T_n} e^{T_n - T} by the same Taylor series, then
 // the downward recursion F_m = (2T F_{m+1} + e^{-T})/(2m+1).  T >= 40: F_0 = sqrt(pi/T)/2
 // (erfc(sqrt(40)) < 1e-18) and the upward recursion F_{m+1} = ((2m+1) F_m - e^{-T})/(2T).
 // Reference: gbasis/integrals/boys_functions.py:26-63 (definition), :102-142 (recursion).
@@ -31,10 +31,10 @@ __device__ __forceinline__ void boys_eval(double T, const double* __restrict__ s
   if (T < kBoysTMax) {
     const int n = __double2int_rn(T * 10.0);
     const double x = fma(-T, 10.0, (double)n) * 0.1;  // T_n - T
-    const double* g = s_tab + n * kBoysTaylor;
-    double f = g[kBoysTaylor - 1];
+    const double* g = s_tab + n;
+    double f = g[(kBoysTaylor - 1) * kBoysNGrid];
 #pragma unroll
-    for (int k = kBoysTaylor - 2; k >= 0; --k) f = fma(f, x, g[k]);
+    for (int k = kBoysTaylor - 2; k >= 0; --k) f = fma(f, x, g[k * kBoysNGrid]);
     F[L] = f;
     if (L > 0) {
       double e = 1.0 / 5040.0;
@@ -85,15 +85,18 @@ __device__ __forceinline__ int internal_count(const ShellDev& s) {
   return (s.sph && s.l >= 2) ? 2 * s.l + 1 : ncart(s.l);
 }
 
-// Stage F_{L+k}(T_n)/k! (k < kBoysTaylor) and e^{-T_n} into shared memory.
+// Stage F_{L+k}(T_n)/k! (k < kBoysTaylor) and e^{-T_n} into shared memory, k-major: the
+// lanes of a warp look up one k at a time at their own grid points n, and consecutive n sit in
+// different banks (an n-major row of 8 doubles would put every n in one of two bank pairs).
 template <int L>
 __device__ __forceinline__ void stage_boys(const double* __restrict__ tab, double* s_tab,
                                            double* s_exp) {
-  constexpr double inv_fact[8] = {1.0, 1.0, 0.5, 1.0 / 6, 1.0 / 24, 1.0 / 120, 1.0 / 720,
-                                  1.0 / 5040};
-  for (int idx = threadIdx.x; idx < kBoysNGrid * kBoysTaylor; idx += blockDim.x) {
-    const int n = idx / kBoysTaylor, k = idx % kBoysTaylor;
-    s_tab[idx] = tab[n * (kBoysOrders + 1) + L + k] * inv_fact[k];
+  double inv_fact = 1.0;  // 1/k!
+#pragma unroll
+  for (int k = 0; k < kBoysTaylor; ++k) {
+    if (k > 1) inv_fact /= k;
+    for (int n = threadIdx.x; n < kBoysNGrid; n += blockDim.x)
+      s_tab[k * kBoysNGrid + n] = tab[n * (kBoysOrders + 1) + L + k] * inv_fact;
   }
   for (int n = threadIdx.x; n < kBoysNGrid; n += blockDim.x)
     s_exp[n] = tab[n * (kBoysOrders + 1) + kBoysOrders];

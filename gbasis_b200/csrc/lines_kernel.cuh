@@ -427,32 +427,148 @@ int launch_lines_t(const EriLaunch& a, const CoopMeta& m, cudaStream_t st) {
   return cuda_status(cudaGetLastError(), "eri_lines launch");
 }
 
+// Per quartet of a split CTA's group: what the tail needs, captured in shared memory while the
+// quartet's pair data are in registers (the tail then makes no dependent global loads for it).
+struct SplitQuartet {
+  double pab[3], qab[3];
+  int shA, shB, shC, shD;
+  int pfo, qfo, mol, bra;
+};
+
+// Row stride of the split kernel's shared accumulators: a row holds NF values of [e0|f0] and,
+// after the ket recursion (done in place), NCD values of [e0|cd]; odd, so that lanes reading
+// consecutive rows hit different banks.
+__host__ __device__ constexpr int split_rs(int nf, int ncd) { return (nf > ncd ? nf : ncd) | 1; }
+
+// Tail of a split CTA's group of nq quartets, spread over all its threads: first tasks (quartet,
+// row e) run the ket horizontal recursion and ket transforms in registers (T::ket) and write
+// [e0|cd] back over the row; then tasks (quartet, output column (c, d)) run the bra recursion
+// (T::bra), bra transforms, scaling and the store (mode 0), or the Schwarz maximum (mode 1).
+template <int LA, int LB, int LC, int LD, class T, int NE, int RS>
+__device__ __forceinline__ void split_tail(const EriLaunch& a, double* ACC,
+                                           const SplitQuartet* sq, unsigned long long* s_mx,
+                                           int nq) {
+  constexpr int NCA = ncart(LA), NCB = ncart(LB), NCC = ncart(LC), NCDD = ncart(LD);
+  constexpr int NCD = NCC * NCDD, NAB = NCA * NCB;
+  constexpr int QS = NE * RS;
+  const bool schwarz = a.mode == 1;
+  for (int t = threadIdx.x; t < nq * NE; t += blockDim.x) {
+    const int q = t / NE, e = t - q * NE;
+    const SplitQuartet& s = sq[q];
+    double* row = ACC + q * QS + e * RS;
+    double h[NCD];
+    T::ket(row, s.qab[0], s.qab[1], s.qab[2], h);
+    if (!schwarz) {
+      if (LD >= 2 && a.shells[s.shD].sph) sph_axis<LD, NCC, 1>(h);
+      if (LC >= 2 && a.shells[s.shC].sph) sph_axis<LC, 1, NCDD>(h);
+    }
+#pragma unroll
+    for (int i = 0; i < NCD; ++i) row[i] = h[i];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nq * NCD; t += blockDim.x) {
+    const int q = t / NCD, k = t - q * NCD;
+    const SplitQuartet& s = sq[q];
+    const ShellDev& sA = a.shells[s.shA];
+    const ShellDev& sB = a.shells[s.shB];
+    const ShellDev& sC = a.shells[s.shC];
+    const ShellDev& sD = a.shells[s.shD];
+    const int nAi = schwarz ? NCA : internal_count(sA), nBi = schwarz ? NCB : internal_count(sB);
+    const int nCi = schwarz ? NCC : internal_count(sC), nDi = schwarz ? NCDD : internal_count(sD);
+    if (k >= nCi * nDi) continue;
+    const int uc = k / nDi, ud = k - uc * nDi;
+    double o[NAB];
+    T::bra(ACC + q * QS + uc * NCDD + ud, RS, s.pab[0], s.pab[1], s.pab[2], o);
+    if (schwarz) {
+      const double wcd = gen::cnorm<LC>(uc) * gen::cnorm<LD>(ud);
+      double mx = 0.0;
+#pragma unroll
+      for (int ia = 0; ia < NCA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NCB; ++ib)
+          mx = fmax(mx, fabs(o[ia * NCB + ib]) * (gen::cnorm<LA>(ia) * gen::cnorm<LB>(ib) * wcd));
+      // non-negative doubles order like their bit patterns
+      atomicMax(s_mx + q, (unsigned long long)__double_as_longlong(mx));
+      continue;
+    }
+    if (LB >= 2 && sB.sph) sph_axis<LB, NCA, 1>(o);
+    if (LA >= 2 && sA.sph) sph_axis<LA, 1, NCB>(o);
+    long long bbase, bcols;
+    if (a.mol_base) {
+      bbase = a.mol_base[s.mol];
+      bcols = a.mol_ncols[s.mol];
+    } else {
+      bbase = a.base;
+      bcols = a.ncols;
+    }
+    const long long nBo = sB.nout, nDo = sD.nout;
+    const double fcd = sC.scl[uc] * sD.scl[ud];
+    double* __restrict__ col = a.out + bbase + s.qfo + sC.pos[uc] * nDo + sD.pos[ud];
+#pragma unroll
+    for (int ia = 0; ia < NCA; ++ia) {
+      if (ia >= nAi) break;
+      const double fa = sA.scl[ia] * fcd;
+      const long long ra = (long long)s.pfo + sA.pos[ia] * nBo;
+#pragma unroll
+      for (int ib = 0; ib < NCB; ++ib) {
+        if (ib >= nBi) break;
+        col[(ra + sB.pos[ib]) * bcols] = o[ia * NCB + ib] * fa * sB.scl[ib];
+      }
+    }
+  }
+  if (schwarz) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < nq; q += blockDim.x)
+      a.qout[sq[q].bra] = sqrt(__longlong_as_double((long long)s_mx[q]));
+  }
+}
+
 // Split register kernel for heavy classes of moderate size: a CTA of S = C::kS warps (4 or 8)
 // takes 32 quartets at a time, thread t of warp r computing part r (a contiguous range of bra
 // rows e) of quartet t's contracted [e0|f0] in registers (generated straight-line recursions,
-// as in the light classes' kernel); the parts meet in shared memory ACC[32][NE*NF] and each
-// warp then runs the register tail for 32 / S of the quartets.  Store (mode 0) and Schwarz
+// as in the light classes' kernel); the parts meet in shared memory ACC[32][NE][RS] and all
+// threads of the CTA then share the group's tail (split_tail).  Store (mode 0) and Schwarz
 // (mode 1) only.
 template <class C>
 __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
   __shared__ double s_tab[kBoysNGrid * kBoysTaylor];
   __shared__ double s_exp[kBoysNGrid];
+  __shared__ SplitQuartet sq[32];
+  __shared__ unsigned long long s_mx[32];
   extern __shared__ double dyn[];
   constexpr int L = C::L;
-  constexpr int NENF = C::NE * C::NF;
   constexpr int NCD = ncart(C::LC) * ncart(C::LD);
+  constexpr int RS = split_rs(C::NF, NCD);
+  constexpr int QS = C::NE * RS;
   stage_boys<L>(a.boys_tab, s_tab, s_exp);
-  __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* ACC = dyn;
-  double* HF = dyn + 32 * NENF + warp * C::NE * NCD;
   const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
   for (long long base = (long long)blockIdx.x * 32; base < count; base += (long long)gridDim.x * 32) {
+    if (threadIdx.x < 32) s_mx[threadIdx.x] = 0ull;
+    __syncthreads();  // Boys table staged (first group); previous group's tail done
     const long long w = base + lane;
     if (w < count) {
       const int2 pq = a.work[a.reverse ? a.work_off + a.nwork - 1 - w : a.work_off + w];
       const PairDev P = a.pairs[pq.x];
       const PairDev Q = a.pairs[pq.y];
+      if (warp == 0) {
+        SplitQuartet& s = sq[lane];
+        s.pab[0] = P.ABx;
+        s.pab[1] = P.ABy;
+        s.pab[2] = P.ABz;
+        s.qab[0] = Q.ABx;
+        s.qab[1] = Q.ABy;
+        s.qab[2] = Q.ABz;
+        s.shA = P.shA;
+        s.shB = P.shB;
+        s.shC = Q.shA;
+        s.shD = Q.shB;
+        s.pfo = P.fo;
+        s.qfo = Q.fo;
+        s.mol = P.mol;
+        s.bra = pq.x;
+      }
       double acc[C::kAcc];
 #pragma unroll
       for (int i = 0; i < C::kAcc; ++i) acc[i] = 0.0;
@@ -478,21 +594,14 @@ __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
         }
       }
       const int nv = C::ne(warp) * C::NF;
-      double* dst = ACC + lane * NENF + C::e0(warp) * C::NF;
+      double* dst = ACC + lane * QS + C::e0(warp) * RS;
 #pragma unroll
       for (int i = 0; i < C::kAcc; ++i)
-        if (i < nv) dst[i] = acc[i];
+        if (i < nv) dst[(i / C::NF) * RS + i % C::NF] = acc[i];
     }
     __syncthreads();
-    for (int q = warp; q < 32; q += C::kS) {
-      const long long wq = base + q;
-      if (wq >= count) break;
-      const int2 pq = a.work[a.reverse ? a.work_off + a.nwork - 1 - wq : a.work_off + wq];
-      const PairDev P = a.pairs[pq.x];
-      const PairDev Q = a.pairs[pq.y];
-      lines_tail<C::LA, C::LB, C::LC, C::LD, typename C::Tail>(a, ACC + q * NENF, HF, pq, P, Q,
-                                                               lane, C::NE, C::NF);
-    }
+    const int nq = (int)(count - base < 32 ? count - base : 32);
+    split_tail<C::LA, C::LB, C::LC, C::LD, typename C::Tail, C::NE, RS>(a, ACC, sq, s_mx, nq);
     __syncthreads();
   }
 }
@@ -500,7 +609,7 @@ __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
 template <class C>
 int launch_split_t(const EriLaunch& a, cudaStream_t st) {
   constexpr int NCD = ncart(C::LC) * ncart(C::LD);
-  const size_t dyn = (size_t)(32 * C::NE * C::NF + C::kS * C::NE * NCD) * sizeof(double);
+  const size_t dyn = (size_t)32 * C::NE * split_rs(C::NF, NCD) * sizeof(double);
   int s = cuda_status(cudaFuncSetAttribute(eri_split<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)dyn), "eri_split shared memory attribute");
   if (s) return s;
