@@ -415,7 +415,22 @@ int launch_lines_t(const EriLaunch& a, const CoopMeta& m, cudaStream_t st) {
   A.m = m;
   size_t smem = 0;
   int wpc = 1;
-  int s = coop_plan(m, (long long)C::kW + C::kY + C::L + 1, A, smem, wpc);
+  int s = GBX_OK;
+  if (C::kRegTail && a.mode != 2) {
+    // register tail: per warp ACC, then W | Y | Boys values, overlaid by the tail's [e0|cd]
+    // rows; no interpreter buffers and no staged programs
+    constexpr long long kNCD = ncart(C::LC) * ncart(C::LD);
+    constexpr long long kPhaseA = (long long)C::kW + C::kY + C::L + 1;
+    constexpr long long kPerWarp =
+        (long long)C::NE * C::NF + (kPhaseA > C::NE * kNCD ? kPhaseA : C::NE * kNCD);
+    A.R = A.Cc = 1;
+    A.prog_doubles = 0;
+    A.smem_per_warp = (int)kPerWarp;
+    wpc = (int)std::max<long long>(1, std::min<long long>(4, kCoopMaxSmem / (kPerWarp * 8)));
+    smem = (size_t)wpc * kPerWarp * 8;
+  } else {
+    s = coop_plan(m, (long long)C::kW + C::kY + C::L + 1, A, smem, wpc);
+  }
   if (s) return s;
   // the Coulomb epilogue (mode 2) is a separate instantiation, so that the store / Schwarz
   // kernel of a class with the register tail carries no interpreted tail
