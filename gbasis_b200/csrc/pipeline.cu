@@ -256,32 +256,59 @@ __device__ __forceinline__ void stage_row(const ExpandArgs& e, long long r, int 
 }
 
 // One N^2 plane from the staged row: dst[c*cs + d] = M[r, gtab[c, d]], cs = N (chemist plane
-// out[x, y, :, :]) or N^2 (physicist out[x, :, y, :]).
+// out[x, y, :, :], contiguous) or N^2 (physicist out[x, :, y, :]); when `mir` is not null the
+// same values also go to the mirror plane there (one table and row read for both stores).
+//   chemist: thread t takes plane elements t, t + T, t + 2T, t + 3T per pass (T threads; table
+//     loads in flight together, each store coalesced across the warp);
+//   physicist: warp w takes the plane rows c = w, w + warps, ...; lane l the columns d = l + 32k,
+//     four per pass, so no element index is divided by N.
+template <bool PHYS>
 __device__ __forceinline__ void write_plane(const ExpandArgs& e, const double* __restrict__ s_row,
-                                            double* __restrict__ dst, bool phys) {
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const long long n = e.n, n2 = n * n;
+                                            double* __restrict__ dst, double* __restrict__ mir) {
   const int* __restrict__ gtab = e.gtab;
-  // four independent elements per thread per step (table loads in flight together); each
-  // of the four stores is coalesced across the warp
-  const unsigned un = (unsigned)n, un2 = (unsigned)n2;
-  for (unsigned t0 = tid; t0 < un2; t0 += 4u * nt) {
-    int g[4];
+  const int n = (int)e.n;
+  if constexpr (!PHYS) {
+    const unsigned nt = blockDim.x, n2 = (unsigned)n * (unsigned)n;
+    for (unsigned t0 = threadIdx.x; t0 < n2; t0 += 4u * nt) {
+      int g[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const unsigned t = t0 + k * nt;
-      g[k] = t < un2 ? __ldg(gtab + t) : 0;
-    }
+      for (int k = 0; k < 4; ++k) {
+        const unsigned t = t0 + k * nt;
+        g[k] = t < n2 ? __ldg(gtab + t) : 0;
+      }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const unsigned t = t0 + k * nt;
-      if (t < un2) {
-        long long o = t;
-        if (phys) {
-          const unsigned c = t / un, d = t - c * un;
-          o = (long long)c * n2 + d;
+      for (int k = 0; k < 4; ++k) {
+        const unsigned t = t0 + k * nt;
+        if (t < n2) {
+          const double v = s_row[g[k]];
+          __stcs(dst + t, v);
+          if (mir) __stcs(mir + t, v);
         }
-        __stcs(dst + o, s_row[g[k]]);
+      }
+    }
+  } else {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const long long cs = (long long)n * n;
+    for (int c = threadIdx.x >> 5; c < n; c += nw) {
+      const int* __restrict__ grow = gtab + (long long)c * n;
+      double* __restrict__ drow = dst + (long long)c * cs;
+      double* __restrict__ mrow = mir ? mir + (long long)c * cs : nullptr;
+      for (int d0 = lane; d0 < n; d0 += 128) {
+        int g[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int d = d0 + 32 * k;
+          g[k] = d < n ? __ldg(grow + d) : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int d = d0 + 32 * k;
+          if (d < n) {
+            const double v = s_row[g[k]];
+            __stcs(drow + d, v);
+            if (mrow) __stcs(mrow + d, v);
+          }
+        }
       }
     }
   }
@@ -293,6 +320,18 @@ __device__ __forceinline__ double* plane_ptr(const ExpandArgs& e, double* base, 
   return phys ? base + x * n * n2 + y * n : base + (x * n + y) * n2;
 }
 
+// Plane (x, y) of a staged row and, when the row's pair has x != y, the mirror plane (y, x).
+__device__ __forceinline__ void write_row_planes(const ExpandArgs& e, const double* s_row,
+                                                 double* base, long long x, long long y,
+                                                 bool mirror, bool phys) {
+  if (phys)
+    write_plane<true>(e, s_row, plane_ptr(e, base, x, y, true),
+                      mirror ? plane_ptr(e, base, y, x, true) : nullptr);
+  else
+    write_plane<false>(e, s_row, plane_ptr(e, base, x, y, false),
+                       mirror ? plane_ptr(e, base, y, x, false) : nullptr);
+}
+
 __global__ void __launch_bounds__(512) expand_rows(const ExpandArgs e) {
   extern __shared__ double s_row[];
   const bool phys = e.notation == GBX_PHYSICIST;
@@ -302,8 +341,7 @@ __global__ void __launch_bounds__(512) expand_rows(const ExpandArgs e) {
     __syncthreads();  // the previous row's planes are written
     stage_row(e, r, ri.w, s_row);
     __syncthreads();
-    write_plane(e, s_row, plane_ptr(e, e.out, ri.x, ri.y, phys), phys);
-    if (ri.z) write_plane(e, s_row, plane_ptr(e, e.out, ri.y, ri.x, phys), phys);
+    write_row_planes(e, s_row, e.out, ri.x, ri.y, ri.z != 0, phys);
   }
 }
 
@@ -354,8 +392,7 @@ __global__ void __launch_bounds__(512) expand_rows_batch(const ExpandArgs* __res
     __syncthreads();
     stage_row(e, r, ri.w, s_row);
     __syncthreads();
-    write_plane(e, s_row, plane_ptr(e, e.out, ri.x, ri.y, phys), phys);
-    if (ri.z) write_plane(e, s_row, plane_ptr(e, e.out, ri.y, ri.x, phys), phys);
+    write_row_planes(e, s_row, e.out, ri.x, ri.y, ri.z != 0, phys);
   }
 }
 
@@ -375,7 +412,8 @@ __global__ void __launch_bounds__(512) expand_slab(const ExpandArgs e, long long
     __syncthreads();
     stage_row(e, r, lr, s_row);
     __syncthreads();
-    write_plane(e, s_row, plane_ptr(e, dst, x - x0, y, phys), phys);
+    if (phys) write_plane<true>(e, s_row, plane_ptr(e, dst, x - x0, y, true), nullptr);
+    else write_plane<false>(e, s_row, plane_ptr(e, dst, x - x0, y, false), nullptr);
   }
 }
 
