@@ -36,9 +36,12 @@ sys.path.insert(0, ROOT)
 WORKLOAD = "medium8"
 METRIC = "unique contracted ERIs/s (FP64 full tensor)"
 UNIT = "ERI/s"
-# DRAM bytes of one expand_rows launch on medium8 from an ncu capture (405.0 MB read +
-# 1,603.4 MB written); the algorithmic bytes are 1,913.5 MB
-EXPAND_TRAFFIC_BYTES = 405.030912e6 + 1603.407e6
+# DRAM bytes of one expand_rows launch on medium8 from an ncu capture (404.8 MB read +
+# 1,599.4 MB written); the algorithmic bytes are 1,913.5 MB
+EXPAND_TRAFFIC_BYTES = 404.778752e6 + 1599.436e6
+
+
+HBM_FALLBACK_GBS = 6650.0  # copy bandwidth measured earlier on this pool's B200s
 
 
 def _peaks():
@@ -396,6 +399,10 @@ def main():
     peak64 = _engine.fp64_peak(local)
     peaks = _peaks()
     hbm = peaks.get("hbm_gbs")
+    hbm_source = "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    if not hbm:
+        # no measured copy bandwidth on this machine: the pool's earlier measurement
+        hbm, hbm_source = HBM_FALLBACK_GBS, "fallback 6650 GB/s copy bandwidth (of fallback)"
     compute_tf = flops / (ph[1] * 1e-3) / 1e12
     exp_bytes = 8.0 * n ** 4 + compact_bytes  # tensor written + compact store read once
     exp_gbs = exp_bytes / (ph[2] * 1e-3) / 1e9
@@ -405,7 +412,7 @@ def main():
                     "traffic": None, "ms": ph[1], "algorithmic_flops": flops}
     roof_expand = {"kernel": "expand_rows", "bound": "hbm", "achieved": exp_gbs, "peak": hbm,
                    "unit": "GB/s", "frac": (exp_gbs / hbm) if hbm else None,
-                   "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                   "peak_source": hbm_source,
                    "traffic": EXPAND_TRAFFIC_BYTES if WORKLOAD == "medium8" else None,
                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                                      "expand_rows launch on this workload (--set full capture)",
