@@ -170,8 +170,21 @@ __device__ __forceinline__ void coulomb_epilogue(const EriLaunch& a, int2 pq, co
 // geometric factors are formed in FP64 and rounded, the vertical and transfer recursions run
 // in FP32, and each primitive quartet's [e0|f0] is added to FP64 accumulators; the
 // horizontal recursion, transforms and stores stay FP64.
+// Resident CTAs per SM a class's register kernel is compiled for.  Classes whose unconstrained
+// register use is 171-200 per thread would fit 2 CTAs of 128 threads per SM; for these the cap
+// of 168 registers that a third CTA needs costs at most a few spilled values, and the extra warps
+// hide more of the primitive-loop latency (measured per class on medium8 and chain20: 8-13 %
+// shorter blocks; classes further above the cap spill heavily and lose).
+__host__ __device__ constexpr int eri_min_blocks(int la, int lb, int lc, int ld) {
+  return ((la == 0 && lb == 2 && lc == 0 && ld == 1) || (la == 1 && lb == 1 && lc == 0 && ld == 1) ||
+          (la == 1 && lb == 3 && lc == 0 && ld == 0))
+             ? 3
+             : 1;
+}
+
 template <int LA, int LB, int LC, int LD, typename R>
-__global__ void __launch_bounds__(kEriThreads) eri_block(const EriLaunch a) {
+__global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
+    eri_block(const EriLaunch a) {
   using C = gen::Cls<LA, LB, LC, LD>;
   constexpr int L = C::L;
   constexpr int NCA = ncart(LA), NCB = ncart(LB), NCC = ncart(LC), NCD = ncart(LD);
