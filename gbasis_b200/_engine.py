@@ -14,7 +14,7 @@ import numpy as np
 from .contractions import is_shell
 
 __all__ = ["lib", "EngineError", "check", "pack_basis", "DeviceBasis", "EXPORTED_SYMBOLS",
-           "library_path", "fp64_peak"]
+           "library_path", "fp64_peak", "release_cached_memory"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libgbx_eri.so")
 
@@ -32,7 +32,7 @@ EXPORTED_SYMBOLS = (
     "gbx_batch_create", "gbx_batch_destroy", "gbx_batch_info", "gbx_batch_run",
     "gbx_batch_set_graph", "gbx_unique_values", "gbx_compact_view",
     "gbx_batch_num_types", "gbx_batch_type_info", "gbx_batch_set_team", "gbx_batch_set_profiling",
-    "gbx_batch_type_times",
+    "gbx_batch_type_times", "gbx_release_cached_memory",
 )
 
 
@@ -101,6 +101,7 @@ def lib():
             "gbx_batch_set_team": [_P, _I, _I],
             "gbx_batch_set_profiling": [_P, _I],
             "gbx_batch_type_times": [_P, _P, _I],
+            "gbx_release_cached_memory": [],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -371,6 +372,11 @@ class DeviceBasis:
             self.close()
         except Exception:
             pass
+
+
+def release_cached_memory():
+    """Free the device memory that closed bases left for reuse (up to 2 GiB per device)."""
+    check(lib().gbx_release_cached_memory(), "gbx_release_cached_memory")
 
 
 def _current_device():

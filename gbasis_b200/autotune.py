@@ -49,10 +49,20 @@ def _key(cls4, avg_prims):
     return "%d%d%d%d:%d" % (*cls4, int(round(math.log2(max(avg_prims, 1.0)))))
 
 
+_loaded = {}  # path -> (modification time, table): read once per change of the file
+
+
 def _load():
+    path = cache_path()
     try:
-        with open(cache_path()) as f:
-            return json.load(f)
+        mtime = os.stat(path).st_mtime_ns
+        hit = _loaded.get(path)
+        if hit and hit[0] == mtime:
+            return dict(hit[1])
+        with open(path) as f:
+            table = json.load(f)
+        _loaded[path] = (mtime, table)
+        return dict(table)
     except (OSError, ValueError):
         return {}
 

@@ -913,8 +913,7 @@ int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStre
   const size_t chunk = (size_t)std::min<long long>(xs, n) * slab;
   if (B.stage_elems < chunk) {
     if (B.d_stage) {
-      cudaFree(B.d_stage);
-      B.dev_allocs.erase(std::find(B.dev_allocs.begin(), B.dev_allocs.end(), (void*)B.d_stage));
+      B.release(B.d_stage);
       B.d_stage = nullptr;
       B.stage_elems = 0;
     }

@@ -100,13 +100,61 @@ struct DeviceGuard {
   }
 };
 
-static void free_dev(void* p) {
-  if (p) cudaFree(p);
+// ------------------------------------------------------------------- block cache
+// Device blocks a basis gives back are kept for the next basis in the process, up to
+// kBlockCacheBytes per device: the public full-tensor call builds and drops a basis every time,
+// and cudaFree (which waits for the whole device) plus cudaMalloc of the compact store and the
+// staging slabs cost milliseconds per call.  A block is reused for a request of at least half
+// its size.  gbx_release_cached_memory() frees the cache.
+constexpr size_t kBlockCacheBytes = size_t(2) << 30;
+struct CachedBlock {
+  int device;
+  void* p;
+  size_t bytes;
+};
+static std::mutex g_block_mu;
+static std::vector<CachedBlock> g_blocks;
+
+static void* cache_take(int device, size_t bytes, size_t* got) {
+  std::lock_guard<std::mutex> lk(g_block_mu);
+  int best = -1;
+  for (int i = 0; i < (int)g_blocks.size(); ++i) {
+    const CachedBlock& b = g_blocks[i];
+    if (b.device != device || b.bytes < bytes || b.bytes / 2 > bytes) continue;
+    if (best < 0 || b.bytes < g_blocks[best].bytes) best = i;
+  }
+  if (best < 0) return nullptr;
+  void* p = g_blocks[best].p;
+  *got = g_blocks[best].bytes;
+  g_blocks.erase(g_blocks.begin() + best);
+  return p;
+}
+
+// The caller has made sure no work on the device still uses p.
+static void cache_give(int device, void* p, size_t bytes) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lk(g_block_mu);
+    size_t held = 0;
+    for (const CachedBlock& b : g_blocks)
+      if (b.device == device) held += b.bytes;
+    if (held + bytes <= kBlockCacheBytes) {
+      g_blocks.push_back({device, p, bytes});
+      return;
+    }
+  }
+  cudaFree(p);
 }
 
 Basis::~Basis() {
   DeviceGuard g(device);
-  for (void* p : dev_allocs) free_dev(p);
+  // blocks go back to the cache only once nothing queued on the device can still use them
+  // (what cudaFree would have waited for)
+  if (cudaDeviceSynchronize() == cudaSuccess) {
+    for (auto& a : dev_allocs) cache_give(device, a.first, a.second);
+  } else {
+    for (auto& a : dev_allocs) cudaFree(a.first);
+  }
   for (cudaEvent_t& e : ev)
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t& e : blk_ev)
@@ -125,16 +173,32 @@ Basis::~Basis() {
 
 int Basis::alloc(void** p, size_t bytes, const char* what) {
   if (bytes == 0) bytes = 16;
-  GBX_CUDA(cudaMalloc(p, bytes), what);
-  dev_allocs.push_back(*p);
+  size_t got = 0;
+  *p = cache_take(device, bytes, &got);
+  if (!*p) {
+    GBX_CUDA(cudaMalloc(p, bytes), what);
+    got = bytes;
+  }
+  dev_allocs.push_back({*p, got});
   return GBX_OK;
+}
+
+void Basis::release(void* p) {
+  for (size_t i = 0; i < dev_allocs.size(); ++i) {
+    if (dev_allocs[i].first != p) continue;
+    // the block may still be read by queued work of this basis: wait for the device, as
+    // cudaFree would
+    if (cudaDeviceSynchronize() == cudaSuccess) cache_give(device, p, dev_allocs[i].second);
+    else cudaFree(p);
+    dev_allocs.erase(dev_allocs.begin() + i);
+    return;
+  }
 }
 
 int Basis::ensure_scratch(size_t compact_elems, size_t work_elems) {
   if (compact_elems > compact_cap) {
     if (d_compact) {
-      cudaFree(d_compact);
-      dev_allocs.erase(std::find(dev_allocs.begin(), dev_allocs.end(), (void*)d_compact));
+      release(d_compact);
       d_compact = nullptr;
     }
     int s = alloc((void**)&d_compact, compact_elems * sizeof(double), "cudaMalloc(compact store)");
@@ -148,8 +212,7 @@ int Basis::ensure_scratch(size_t compact_elems, size_t work_elems) {
 int Basis::ensure_out(size_t elems) {
   if (elems <= out_cap) return GBX_OK;
   if (d_out) {
-    cudaFree(d_out);
-    dev_allocs.erase(std::find(dev_allocs.begin(), dev_allocs.end(), (void*)d_out));
+    release(d_out);
     d_out = nullptr;
     out_cap = 0;
   }
@@ -371,6 +434,19 @@ int coulomb_entry(gbx_basis* b, const double* D, double tau, double* J, cudaStre
 }  // namespace gbx
 
 extern "C" {
+
+int gbx_release_cached_memory(void) {
+  std::vector<CachedBlock> blocks;
+  {
+    std::lock_guard<std::mutex> lk(g_block_mu);
+    blocks.swap(g_blocks);
+  }
+  for (const CachedBlock& b : blocks) {
+    DeviceGuard g(b.device);
+    cudaFree(b.p);
+  }
+  return GBX_OK;
+}
 
 int gbx_last_error(char* buf, size_t len) {
   if (!buf || len == 0) return GBX_ERR_INVALID;

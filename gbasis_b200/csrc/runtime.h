@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <utility>
 #include <vector>
 
 #include "errors.h"
@@ -97,10 +98,11 @@ struct Basis {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t stage_ready[kStageBuffers] = {};
   cudaEvent_t stage_free[kStageBuffers] = {};
-  std::vector<void*> dev_allocs;
+  std::vector<std::pair<void*, size_t>> dev_allocs;  // every device block the basis holds
 
   ~Basis();
   int alloc(void** p, size_t bytes, const char* what);
+  void release(void* p);  // give one block back (to the process's block cache)
   int ensure_scratch(size_t compact_elems, size_t work_elems);
   int ensure_out(size_t elems);
 };

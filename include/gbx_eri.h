@@ -197,6 +197,12 @@ int gbx_block_info(const gbx_basis* b, int k, int* cls4, int* team, double* avg_
 int gbx_set_team(gbx_basis* b, int k, int team);
 int gbx_block_times(gbx_basis* b, double* ms, int n);
 
+/* Device memory that destroyed bases gave back is kept (up to 2 GiB per device) for the next
+ * basis of the process: the full-tensor call of the Python layer (the replacement of
+ * gbasis/integrals/electron_repulsion.py:214-281, which allocates per call) builds and drops a
+ * basis every time.  This frees that cache on every device. */
+int gbx_release_cached_memory(void);
+
 /* Copy of the last error message on this thread (NUL-terminated, truncated to len). */
 int gbx_last_error(char* buf, size_t len);
 
