@@ -11,6 +11,7 @@ using namespace gbx;
 
 namespace gbx {
 int coulomb_entry(gbx_basis* b, const double* D, double tau, double* J, cudaStream_t st);
+int jk_entry(gbx_basis* b, const double* D, double tau, double* J, double* K, cudaStream_t st);
 }
 
 namespace {
@@ -108,6 +109,13 @@ int gbx_eri_coulomb_j(gbx_basis* b, const double* D, double tau, double* J, void
   if (!b || !D || !J) return set_error(GBX_ERR_INVALID, "gbx_eri_coulomb_j: null argument");
   if (!(tau >= 0.0)) return set_error(GBX_ERR_INVALID, "schwarz threshold must be >= 0");
   return gbx::coulomb_entry(b, D, tau, J, (cudaStream_t)stream);
+}
+
+int gbx_eri_jk(gbx_basis* b, const double* D, double tau, double* J, double* K, void* stream) {
+  if (!b || !D || !J || !K) return set_error(GBX_ERR_INVALID, "gbx_eri_jk: null argument");
+  if (J == K) return set_error(GBX_ERR_INVALID, "gbx_eri_jk: J and K must be different buffers");
+  if (!(tau >= 0.0)) return set_error(GBX_ERR_INVALID, "schwarz threshold must be >= 0");
+  return gbx::jk_entry(b, D, tau, J, K, (cudaStream_t)stream);
 }
 
 }  // extern "C"

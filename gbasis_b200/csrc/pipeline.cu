@@ -345,6 +345,86 @@ __global__ void __launch_bounds__(512) expand_rows(const ExpandArgs e) {
   }
 }
 
+// Element (p, q) of the compact matrix M of unique integrals (p, q pair functions), read from
+// global memory: the block (X, Y) with X > Y, or with X == Y and p's local pair index >= q's,
+// holds it at row p, column q; otherwise it sits transposed in block (Y, X).
+__device__ __forceinline__ double compact_at(const ExpandArgs& e, long long p, int X,
+                                             long long rp, int lp, long long q) {
+  int Y = 0;
+  while (q >= e.pf_first[Y + 1]) ++Y;
+  const long long rq = q - e.pf_first[Y];
+  const int lq = __ldg(&e.rowinfo[q].w);
+  (void)p;
+  if (X > Y || (X == Y && lp >= lq)) {
+    const BlockDev bd = e.blocks[X * kNumPairClasses + Y];
+    return __ldg(e.compact + bd.base + rp * bd.ncols + rq);
+  }
+  const BlockDev bd = e.blocks[Y * kNumPairClasses + X];
+  return __ldg(e.compact + bd.base + rq * bd.ncols + rp);
+}
+
+// Coulomb and exchange matrices from the compact store.  Row r of M (the pair function of the
+// ordered function pairs (x, y) and, when x != y, (y, x)) holds (xy|cd) for every (c, d)
+// through gtab, so
+//   J[x][y] = J[y][x] = sum_cd (xy|cd) D[c][d],
+//   K[x][c] += sum_d (xy|cd) D[y][d],   K[y][c] += sum_d (xy|cd) D[x][d]  (x != y).
+// Every ordered pair belongs to exactly one row: J is stored, K (cleared by the caller) summed
+// with atomics, 2N per row.  Warp w takes the plane rows c = w, w + warps, ...; lanes take d.
+// STAGED: the row is gathered into shared memory first (as expand_rows does); otherwise each
+// element is read from the compact store (rows larger than shared memory).
+template <bool STAGED>
+__global__ void __launch_bounds__(512) jk_rows(const ExpandArgs e, const double* __restrict__ D,
+                                               double* __restrict__ J, double* __restrict__ K) {
+  extern __shared__ double s_row[];
+  __shared__ double s_j[16];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int n = (int)e.n;
+  for (long long r = blockIdx.x; r < e.npf; r += gridDim.x) {
+    const int4 ri = __ldg(e.rowinfo + r);
+    if (ri.x < 0) continue;
+    int X = 0;
+    while (r >= e.pf_first[X + 1]) ++X;
+    const long long rp = r - e.pf_first[X];
+    __syncthreads();  // the previous row's shared values are read
+    if constexpr (STAGED) stage_row(e, r, ri.w, s_row);
+    __syncthreads();
+    const double* __restrict__ Dx = D + (long long)ri.x * n;
+    const double* __restrict__ Dy = D + (long long)ri.y * n;
+    double jp = 0.0;
+    for (int c = warp; c < n; c += nw) {
+      const int* __restrict__ grow = e.gtab + (long long)c * n;
+      const double* __restrict__ Dc = D + (long long)c * n;
+      double kx = 0.0, ky = 0.0;
+      for (int d = lane; d < n; d += 32) {
+        const int g = __ldg(grow + d);
+        double v;
+        if constexpr (STAGED) v = s_row[g];
+        else v = compact_at(e, r, X, rp, ri.w, g);
+        jp = fma(v, __ldg(Dc + d), jp);
+        kx = fma(v, __ldg(Dy + d), kx);
+        ky = fma(v, __ldg(Dx + d), ky);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        kx += __shfl_xor_sync(0xffffffffu, kx, o);
+        ky += __shfl_xor_sync(0xffffffffu, ky, o);
+      }
+      if (lane == 0) {
+        atomicAdd(K + (long long)ri.x * n + c, kx);
+        if (ri.z) atomicAdd(K + (long long)ri.y * n + c, ky);
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) jp += __shfl_xor_sync(0xffffffffu, jp, o);
+    if (lane == 0) s_j[warp] = jp;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < nw; ++w) t += s_j[w];
+      J[(long long)ri.x * n + ri.y] = t;
+      if (ri.z) J[(long long)ri.y * n + ri.x] = t;
+    }
+  }
+}
+
 // (ab|cd) of n function quadruples (a, b, c, d) from the compact store (indices checked by
 // the host to be below N).
 __global__ void gather_unique(const ExpandArgs e, const long long* __restrict__ idx4, long long n,
@@ -1039,6 +1119,30 @@ int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, d
     expand_full<<<grid, 256, 0, st>>>(e);
     GBX_CUDA(cudaGetLastError(), "expand_full launch");
   }
+  if (B.profiling) cudaEventRecord(B.ev[3], st);
+  return GBX_OK;
+}
+
+// J and K of a density from the unique integrals (compact store; the N^4 tensor is never
+// formed).  D, J, K: device N x N row-major.
+int run_jk(Basis& B, const double* D, double tau, double* J, double* K, cudaStream_t st) {
+  int s = run_compact(B, tau, st, 0.0, 0.0);
+  if (s) return s;
+  const ExpandArgs e = expand_args(B, GBX_CHEMIST, nullptr);
+  GBX_CUDA(cudaMemsetAsync(K, 0, (size_t)B.nbf * B.nbf * sizeof(double), st), "clear K");
+  if (B.profiling) cudaEventRecord(B.ev[2], st);  // the contraction takes the expansion's slot
+  const size_t row_bytes = (size_t)e.npf * sizeof(double);
+  int per_sm = 0;
+  if ((s = row_kernel_fit(B.device, jk_rows<true>, row_bytes, &per_sm))) return s;
+  const int nsm = num_sms(B.device);
+  if (per_sm > 0) {
+    const int grid = (int)std::max<long long>(1, std::min<long long>(e.npf, (long long)nsm * per_sm));
+    jk_rows<true><<<grid, 512, row_bytes, st>>>(e, D, J, K);
+  } else {
+    const int grid = (int)std::max<long long>(1, std::min<long long>(e.npf, (long long)nsm * 4));
+    jk_rows<false><<<grid, 512, 0, st>>>(e, D, J, K);
+  }
+  if ((s = cuda_status(cudaGetLastError(), "jk_rows launch"))) return s;
   if (B.profiling) cudaEventRecord(B.ev[3], st);
   return GBX_OK;
 }

@@ -431,6 +431,11 @@ int coulomb_entry(gbx_basis* b, const double* D, double tau, double* J, cudaStre
   DeviceGuard g(B.device);
   return run_coulomb(B, D, tau, J, st);
 }
+int jk_entry(gbx_basis* b, const double* D, double tau, double* J, double* K, cudaStream_t st) {
+  Basis& B = *b->impl;
+  DeviceGuard g(B.device);
+  return run_jk(B, D, tau, J, K, st);
+}
 }  // namespace gbx
 
 extern "C" {

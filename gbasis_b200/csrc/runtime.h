@@ -117,6 +117,7 @@ int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, d
 int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStream_t st);
 int run_compact(Basis& B, double tau, cudaStream_t st, double skip = 0.0, double fp32 = 0.0);
 int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st);
+int run_jk(Basis& B, const double* D, double tau, double* J, double* K, cudaStream_t st);
 int ensure_schwarz(Basis& B, cudaStream_t st);
 int unique_values(Basis& B, long long n, const long long* idx4_host, double* out_host,
                   cudaStream_t st);

@@ -24,6 +24,8 @@
  *                                   (gbasis/base_four_symm.py:559-616)
  *   - gbx_eri_coulomb_j          <- (no direct counterpart: J_ab = sum_cd (ab|cd) D_cd,
  *                                   the contraction gbasis users apply to the tensor)
+ *   - gbx_eri_jk                 <- (no direct counterpart: J and K_ac = sum_bd (ab|cd) D_bd
+ *                                   from the same tensor)
  */
 #ifndef GBX_ERI_H
 #define GBX_ERI_H
@@ -176,6 +178,15 @@ int gbx_batch_type_times(gbx_batch* b, double* ms, int n);
  * (full tensor never stored).  D, J: device N x N row-major (D symmetric). */
 int gbx_eri_coulomb_j(gbx_basis* b, const double* D, double schwarz_threshold, double* J,
                       void* stream);
+
+/* Coulomb and exchange matrices of a density D (any N x N, not only symmetric):
+ *   J[a,b] = sum_cd (ab|cd) D[c,d],   K[a,c] = sum_bd (ab|cd) D[b,d]   (chemist notation),
+ * from the unique integrals of the screened quartets (the N^4 tensor is never formed; the
+ * unique-integral store, N^4/8 values, is).  No gbasis counterpart: gbasis users contract the
+ * tensor of electron_repulsion_integral (gbasis/integrals/electron_repulsion.py:214-281) this
+ * way.  D, J, K: device N x N row-major, three different buffers. */
+int gbx_eri_jk(gbx_basis* b, const double* D, double schwarz_threshold, double* J, double* K,
+               void* stream);
 
 /* Device-side counters of the last call on this basis: quartets computed and screened. */
 int gbx_last_counts(const gbx_basis* b, int64_t* computed, int64_t* screened);

@@ -1,10 +1,12 @@
-"""Direct Coulomb matrix (through the C ABI) against the contraction of the full tensor."""
+"""Direct Coulomb matrix, and Coulomb plus exchange from the unique integrals (through the C
+ABI), against the contractions of the full tensor."""
 import numpy as np
 import pytest
 
 from conftest import load_npz, shells_from_json
 from gbasis_b200 import electron_repulsion as er
-from gbasis_b200.coulomb import coulomb_matrix
+from gbasis_b200 import _engine
+from gbasis_b200.coulomb import coulomb_exchange, coulomb_matrix
 from gbasis_b200.synthetic import density_matrix, make_workload
 
 pytestmark = pytest.mark.gpu
@@ -37,3 +39,89 @@ def test_coulomb_mixed_with_f_shells():
 
 def test_coulomb_medium8():
     _check(make_workload("medium8")[:18], 1e-8)
+
+
+def _check_jk(shells, thr, symmetric):
+    eri = er.electron_repulsion_integral(shells, notation="chemist")
+    n = eri.shape[0]
+    rng = np.random.default_rng(n)
+    D = rng.standard_normal((n, n))
+    if symmetric:
+        D = D + D.T
+    J, K = coulomb_exchange(shells, D)
+    Jr, Kr = np.einsum("abcd,cd->ab", eri, D), np.einsum("abcd,bd->ac", eri, D)
+    tol = 1e-12 * max(1.0, np.abs(Jr).max(), np.abs(Kr).max())
+    np.testing.assert_allclose(J, Jr, rtol=0, atol=tol)
+    np.testing.assert_allclose(K, Kr, rtol=0, atol=tol)
+    if thr:
+        eri_t = er.electron_repulsion_integral_improved(shells, notation="chemist",
+                                                        schwarz_threshold=thr)
+        Jt, Kt = coulomb_exchange(shells, D, schwarz_threshold=thr)
+        np.testing.assert_allclose(Jt, np.einsum("abcd,cd->ab", eri_t, D), rtol=0, atol=tol)
+        np.testing.assert_allclose(Kt, np.einsum("abcd,bd->ac", eri_t, D), rtol=0, atol=tol)
+
+
+def test_jk_tiny4_general_density():
+    _check_jk(make_workload("tiny4"), 1e-4, symmetric=False)
+
+
+def test_jk_mixed_with_f_shells():
+    z = load_npz("mixed.npz")
+    _check_jk(shells_from_json(z["shells"]), 1e-3, symmetric=True)
+
+
+def test_jk_medium8_subset():
+    _check_jk(make_workload("medium8")[:18], 0.0, symmetric=False)
+
+
+def test_jk_rows_beyond_shared_memory():
+    """255 functions: a row of unique integrals (32,640 values) exceeds shared memory, so the
+    kernel reads the compact store directly; reference contractions of the device tensor."""
+    import torch
+    from gbasis_b200.synthetic import box_atoms, random_shell
+    rng = np.random.default_rng(77)
+    recipe = [(0, 6), (0, 3), (0, 1), (1, 3), (1, 1), (2, 1)]
+    shells = [random_shell(rng, l, k, c, "cartesian") for c in box_atoms(rng, 17, 13.0)
+              for l, k in recipe]
+    db = _engine.DeviceBasis(shells)
+    try:
+        n = db.nbf
+        assert n * (n + 1) // 2 * 8 > 227 * 1024
+        g = torch.Generator(device="cuda").manual_seed(5)
+        D = torch.randn((n, n), dtype=torch.float64, device="cuda", generator=g)
+        T = torch.empty(n ** 4, dtype=torch.float64, device="cuda")
+        db.full_device(T.data_ptr(), "chemist")   # [a, b, c, d]
+        Jr = (T.view(n * n, n * n) @ D.reshape(-1)).view(n, n)
+        db.full_device(T.data_ptr(), "physicist")  # [a, c, b, d]
+        Kr = (T.view(n * n, n * n) @ D.reshape(-1)).view(n, n)
+        del T
+        J = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        K = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        _engine.check(_engine.lib().gbx_eri_jk(db.handle, D.data_ptr(), 0.0, J.data_ptr(),
+                                               K.data_ptr(), None), "gbx_eri_jk")
+        torch.cuda.synchronize()
+        tol = 1e-12 * max(1.0, float(Jr.abs().max()), float(Kr.abs().max()))
+        assert float((J - Jr).abs().max()) <= tol
+        assert float((K - Kr).abs().max()) <= tol
+    finally:
+        db.close()
+        torch.cuda.empty_cache()
+
+
+def test_jk_rejects_bad_arguments():
+    import torch
+    db = _engine.DeviceBasis(make_workload("tiny4"))
+    try:
+        n = db.nbf
+        D, J = (torch.zeros((n, n), dtype=torch.float64, device="cuda") for _ in range(2))
+        L = _engine.lib()
+        with pytest.raises(ValueError):
+            _engine.check(L.gbx_eri_jk(db.handle, D.data_ptr(), 0.0, J.data_ptr(), 0, None))
+        with pytest.raises(ValueError):
+            _engine.check(L.gbx_eri_jk(db.handle, D.data_ptr(), 0.0, J.data_ptr(), J.data_ptr(),
+                                       None))
+        with pytest.raises(ValueError):
+            _engine.check(L.gbx_eri_jk(db.handle, D.data_ptr(), -1.0, J.data_ptr(),
+                                       D.data_ptr(), None))
+    finally:
+        db.close()
