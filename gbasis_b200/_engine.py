@@ -32,7 +32,7 @@ EXPORTED_SYMBOLS = (
     "gbx_batch_create", "gbx_batch_destroy", "gbx_batch_info", "gbx_batch_run",
     "gbx_batch_set_graph", "gbx_unique_values", "gbx_compact_view",
     "gbx_batch_num_types", "gbx_batch_type_info", "gbx_batch_set_team", "gbx_batch_set_profiling",
-    "gbx_batch_type_times", "gbx_release_cached_memory", "gbx_eri_jk",
+    "gbx_batch_type_times", "gbx_release_cached_memory", "gbx_eri_jk", "gbx_point_charge",
 )
 
 
@@ -103,6 +103,7 @@ def lib():
             "gbx_batch_type_times": [_P, _P, _I],
             "gbx_release_cached_memory": [],
             "gbx_eri_jk": [_P, _P, _D, _P, _P, _P],
+            "gbx_point_charge": [_P, _I, _P, _P, _I, _P, _P],
         }
         for name, args in sig.items():
             f = getattr(L, name)

@@ -41,7 +41,7 @@ def sources(lmax):
     gen = gen_eri.emit_sources(GEN, lmax)
     return [os.path.join(GEN, g) for g in gen] + [
         os.path.join(CSRC, f) for f in ("runtime.cu", "pipeline.cu", "extras.cu", "noalloc.cu",
-                                        "coop_kernel.cu", "batch.cu")]
+                                        "coop_kernel.cu", "batch.cu", "one_elec.cu")]
 
 
 KERNEL_DEPS = ("gbx_common.cuh", "eri_kernels.cuh", "errors.h", "_gen/eri_gen.cuh")
@@ -55,7 +55,8 @@ LINES_DEPS = ("gbx_common.cuh", "errors.h", "coop.cuh", "coop_tail.cuh", "lines_
 def _deps_mtime(src):
     base = os.path.basename(src)
     deps = (KERNEL_DEPS if base.startswith("eri_cls") else
-            LINES_DEPS if base.startswith("lines_") else HOST_DEPS)
+            LINES_DEPS if base.startswith("lines_") else
+            KERNEL_DEPS + HOST_DEPS if base == "one_elec.cu" else HOST_DEPS)
     m = os.path.getmtime(os.path.join(ROOT, "include", "gbx_eri.h"))
     for d in deps:
         p = os.path.join(CSRC, d)

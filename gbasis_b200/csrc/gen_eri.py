@@ -396,7 +396,9 @@ def emit_sources(outdir, lmax):
     every = canonical_classes(lmax)
     light = [c for c in every if is_light(c)]
     heavy = [c for c in every if not is_light(c)]
-    put("eri_gen.cuh", emit_all(lmax, light))
+    # the point-charge kernel uses the (ab|ss) structs of every pair class, heavy ones included
+    one_e = [(la, lb, 0, 0) for la in range(lmax + 1) for lb in range(lmax + 1)]
+    put("eri_gen.cuh", emit_all(lmax, light + [c for c in one_e if c not in light]))
     gen_coop.emit(heavy, os.path.join(outdir, "coop_programs.cuh"))
     files = []
     # spread the light classes over translation units of similar compile cost (code size)

@@ -345,16 +345,16 @@ __global__ void __launch_bounds__(512) expand_rows(const ExpandArgs e) {
   }
 }
 
-// Element (p, q) of the compact matrix M of unique integrals (p, q pair functions), read from
-// global memory: the block (X, Y) with X > Y, or with X == Y and p's local pair index >= q's,
-// holds it at row p, column q; otherwise it sits transposed in block (Y, X).
-__device__ __forceinline__ double compact_at(const ExpandArgs& e, long long p, int X,
-                                             long long rp, int lp, long long q) {
+// Element (p, q) of the compact matrix M of unique integrals (p, q pair functions; p of class X,
+// rp its row within the class, lp its local pair index), read from global memory: the block
+// (X, Y) with X > Y, or with X == Y and lp >= q's local pair index, holds it at row p, column q;
+// otherwise it sits transposed in block (Y, X).
+__device__ __forceinline__ double compact_at(const ExpandArgs& e, int X, long long rp, int lp,
+                                             long long q) {
   int Y = 0;
   while (q >= e.pf_first[Y + 1]) ++Y;
   const long long rq = q - e.pf_first[Y];
   const int lq = __ldg(&e.rowinfo[q].w);
-  (void)p;
   if (X > Y || (X == Y && lp >= lq)) {
     const BlockDev bd = e.blocks[X * kNumPairClasses + Y];
     return __ldg(e.compact + bd.base + rp * bd.ncols + rq);
@@ -399,7 +399,7 @@ __global__ void __launch_bounds__(512) jk_rows(const ExpandArgs e, const double*
         const int g = __ldg(grow + d);
         double v;
         if constexpr (STAGED) v = s_row[g];
-        else v = compact_at(e, r, X, rp, ri.w, g);
+        else v = compact_at(e, X, rp, ri.w, g);
         jp = fma(v, __ldg(Dc + d), jp);
         kx = fma(v, __ldg(Dy + d), kx);
         ky = fma(v, __ldg(Dx + d), ky);

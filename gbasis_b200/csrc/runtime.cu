@@ -436,6 +436,12 @@ int jk_entry(gbx_basis* b, const double* D, double tau, double* J, double* K, cu
   DeviceGuard g(B.device);
   return run_jk(B, D, tau, J, K, st);
 }
+int point_charge_entry(gbx_basis* b, int npoints, const double* coords, const double* charges,
+                       int sum, double* out, cudaStream_t st) {
+  Basis& B = *b->impl;
+  DeviceGuard g(B.device);
+  return run_point_charge(B, npoints, coords, charges, sum, out, st);
+}
 }  // namespace gbx
 
 extern "C" {

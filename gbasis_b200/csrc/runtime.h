@@ -118,6 +118,8 @@ int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStre
 int run_compact(Basis& B, double tau, cudaStream_t st, double skip = 0.0, double fp32 = 0.0);
 int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st);
 int run_jk(Basis& B, const double* D, double tau, double* J, double* K, cudaStream_t st);
+int run_point_charge(Basis& B, int npoints, const double* coords, const double* charges,
+                     int sum, double* out, cudaStream_t st);
 int ensure_schwarz(Basis& B, cudaStream_t st);
 int unique_values(Basis& B, long long n, const long long* idx4_host, double* out_host,
                   cudaStream_t st);

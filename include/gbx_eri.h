@@ -26,6 +26,9 @@
  *                                   the contraction gbasis users apply to the tensor)
  *   - gbx_eri_jk                 <- (no direct counterpart: J and K_ac = sum_bd (ab|cd) D_bd
  *                                   from the same tensor)
+ *   - gbx_point_charge           <- point_charge_integral / nuclear_electron_attraction_integral
+ *                                   (gbasis/integrals/point_charge.py:271-325,
+ *                                    nuclear_electron_attraction.py:8-42)
  */
 #ifndef GBX_ERI_H
 #define GBX_ERI_H
@@ -207,6 +210,15 @@ int gbx_block_info(const gbx_basis* b, int k, int* cls4, int* team, double* avg_
                    int64_t* n_quartets);
 int gbx_set_team(gbx_basis* b, int k, int team);
 int gbx_block_times(gbx_basis* b, double* ms, int n);
+
+/* Point-charge interaction integrals of the basis's functions (the replacement of
+ * point_charge_integral, gbasis/integrals/point_charge.py:271-325, and with sum_points = 1 of
+ * nuclear_electron_attraction_integral, gbasis/integrals/nuclear_electron_attraction.py:8-42):
+ *   sum_points = 0: out[(a*N + b)*n_points + c] = -charges[c] (a| 1/|r - R_c| |b)
+ *   sum_points = 1: out[a*N + b] = sum_c -charges[c] (a| 1/|r - R_c| |b)
+ * coords: host n_points x 3, charges: host n_points (finite); out: device, row-major. */
+int gbx_point_charge(gbx_basis* b, int n_points, const double* coords, const double* charges,
+                     int sum_points, double* out, void* stream);
 
 /* Device memory that destroyed bases gave back is kept (up to 2 GiB per device) for the next
  * basis of the process: the full-tensor call of the Python layer (the replacement of
