@@ -33,6 +33,7 @@ EXPORTED_SYMBOLS = (
     "gbx_batch_set_graph", "gbx_unique_values", "gbx_compact_view",
     "gbx_batch_num_types", "gbx_batch_type_info", "gbx_batch_set_team", "gbx_batch_set_profiling",
     "gbx_batch_type_times", "gbx_release_cached_memory", "gbx_eri_jk", "gbx_point_charge",
+    "gbx_basis_set_potential",
 )
 
 
@@ -104,6 +105,7 @@ def lib():
             "gbx_release_cached_memory": [],
             "gbx_eri_jk": [_P, _P, _D, _P, _P, _P],
             "gbx_point_charge": [_P, _I, _P, _P, _I, _P, _P],
+            "gbx_basis_set_potential": [_P, _I, _D],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -363,6 +365,11 @@ class DeviceBasis:
         a, b = ctypes.c_int64(), ctypes.c_int64()
         check(lib().gbx_last_counts(self.handle, ctypes.byref(a), ctypes.byref(b)))
         return int(a.value), int(b.value)
+
+    def set_potential(self, potential=0, omega=0.0):
+        """Operator of later integral calls: 0 = 1/r, 1 = erf(omega r)/r, 2 = erfc(omega r)/r."""
+        check(lib().gbx_basis_set_potential(self.handle, int(potential), float(omega)),
+              "gbx_basis_set_potential")
 
     def close(self):
         if getattr(self, "handle", None):

@@ -72,7 +72,8 @@ __global__ void eri_coop(const CoopArgs A) {
         const double CEx = fma(ze, bp.Xx, kp.Xx), CEy = fma(ze, bp.Xy, kp.Xy),
                      CEz = fma(ze, bp.Xz, kp.Xz);
         __syncwarp();
-        boys_lanes(M.L, lane, T, bp.C * kp.C * r, a.boys_tab, X);
+        boys_lanes(M.L, lane, T, bp.C * kp.C * r, a.boys_tab, X, a.potential, a.omega,
+                   bp.zeta * rz);
         __syncwarp();
         for (int l = 0; l < M.v_nlv; ++l) {
           const int b = kCoopLv[M.v_lv + l], e = kCoopLv[M.v_lv + l + 1];

@@ -91,14 +91,12 @@ __device__ __forceinline__ int n_int(const ShellDev& s) {
 // Lane m <= L writes pref * F_m(T) to X[m]: T < 40 by the 8-term Taylor expansion of F_m
 // around the nearest grid point (orders m..m+7 of the table), T >= 40 by F_0 = sqrt(pi/T)/2
 // and m upward steps F_{k+1} = ((2k+1) F_k - e^{-T})/(2T).
-__device__ __forceinline__ void boys_lanes(int L, int lane, double T, double pref,
-                                           const double* __restrict__ tab, double* X) {
-  if (lane > L) return;
+__device__ __forceinline__ double boys_lane_value(int m, double T, const double* __restrict__ tab) {
   double f;
   if (T < kBoysTMax) {
     const int n = __double2int_rn(T * 10.0);
     const double x = fma(-T, 10.0, (double)n) * 0.1;
-    const double* g = tab + n * (kBoysOrders + 1) + lane;
+    const double* g = tab + n * (kBoysOrders + 1) + m;
     f = g[7] * (1.0 / 5040);
     f = fma(f, x, g[6] * (1.0 / 720));
     f = fma(f, x, g[5] * (1.0 / 120));
@@ -110,10 +108,29 @@ __device__ __forceinline__ void boys_lanes(int L, int lane, double T, double pre
   } else {
     const double r = rsqrt(T);
     f = 0.88622692545275801365 * r;
-    if (lane > 0) {
+    if (m > 0) {
       const double emT = exp(-T), o2T = 0.5 * r * r;
-      for (int m = 0; m < lane; ++m) f = fma((double)(2 * m + 1), f, -emT) * o2T;
+      for (int k = 0; k < m; ++k) f = fma((double)(2 * k + 1), f, -emT) * o2T;
     }
+  }
+  return f;
+}
+
+// Lane m <= L writes pref * F_m(T) to X[m]; for the range-separated operators (potential 1:
+// erf(omega r)/r, 2: erfc(omega r)/r; gbasis/integrals/boys_functions.py:145-223) the values
+// s^{m+1/2} F_m(s T), s = omega^2 / (omega^2 + rho), or the Coulomb value minus those.
+__device__ __forceinline__ void boys_lanes(int L, int lane, double T, double pref,
+                                           const double* __restrict__ tab, double* X,
+                                           int potential = 0, double omega = 0.0,
+                                           double rho = 0.0) {
+  if (lane > L) return;
+  double f = boys_lane_value(lane, T, tab);
+  if (potential) {
+    const double w2 = omega * omega, sc = w2 / (w2 + rho);
+    double s = sqrt(sc);
+    for (int k = 0; k < lane; ++k) s *= sc;
+    const double g = boys_lane_value(lane, sc * T, tab) * s;
+    f = potential == 1 ? g : f - g;
   }
   X[lane] = f * pref;
 }

@@ -62,6 +62,71 @@ __device__ __forceinline__ void boys_eval(double T, const double* __restrict__ s
   }
 }
 
+// F[m] += c0 sc^m F_m(T) for m = 0..L: the Boys values of one argument folded into F as the
+// recursion produces them (one value live at a time).
+template <int L>
+__device__ __forceinline__ void boys_accumulate(double T, const double* __restrict__ s_tab,
+                                                const double* __restrict__ s_exp, double c0,
+                                                double sc, double* F) {
+  if (T < kBoysTMax) {
+    const int n = __double2int_rn(T * 10.0);
+    const double x = fma(-T, 10.0, (double)n) * 0.1;
+    const double* g = s_tab + n;
+    double f = g[(kBoysTaylor - 1) * kBoysNGrid];
+#pragma unroll
+    for (int k = kBoysTaylor - 2; k >= 0; --k) f = fma(f, x, g[k * kBoysNGrid]);
+    double c = c0;
+#pragma unroll
+    for (int m = 0; m < L; ++m) c *= sc;
+    F[L] = fma(c, f, F[L]);
+    if (L > 0) {
+      double e = 1.0 / 5040.0;
+      e = fma(e, x, 1.0 / 720.0);
+      e = fma(e, x, 1.0 / 120.0);
+      e = fma(e, x, 1.0 / 24.0);
+      e = fma(e, x, 1.0 / 6.0);
+      e = fma(e, x, 0.5);
+      e = fma(e, x, 1.0);
+      e = fma(e, x, 1.0);
+      const double emT = s_exp[n] * e, t2 = 2.0 * T, isc = 1.0 / sc;
+#pragma unroll
+      for (int m = L - 1; m >= 0; --m) {
+        f = fma(t2, f, emT) * inv_odd(m);
+        c *= isc;
+        F[m] = fma(c, f, F[m]);
+      }
+    }
+  } else {
+    const double r = rsqrt(T);
+    double f = 0.88622692545275801365 * r, c = c0;
+    F[0] = fma(c, f, F[0]);
+    if (L > 0) {
+      const double emT = exp(-T), o2T = 0.5 * r * r;
+#pragma unroll
+      for (int m = 0; m < L; ++m) {
+        f = fma((double)(2 * m + 1), f, -emT) * o2T;
+        c *= sc;
+        F[m + 1] = fma(c, f, F[m + 1]);
+      }
+    }
+  }
+}
+
+// Range-separated operators (gbasis/integrals/boys_functions.py:145-223): for erf(omega r)/r
+// the Boys values become s^{m+1/2} F_m(s T), s = omega^2 / (omega^2 + rho); erfc(omega r)/r
+// takes the Coulomb values minus those.  F holds F_m(T) on entry.
+template <int L>
+__device__ __forceinline__ void boys_attenuate(int potential, double omega, double rho, double T,
+                                               const double* __restrict__ s_tab,
+                                               const double* __restrict__ s_exp, double* F) {
+  const double w2 = omega * omega, sc = w2 / (w2 + rho);
+  if (potential == 1) {
+#pragma unroll
+    for (int m = 0; m <= L; ++m) F[m] = 0.0;
+  }
+  boys_accumulate<L>(sc * T, s_tab, s_exp, potential == 1 ? sqrt(sc) : -sqrt(sc), sc, F);
+}
+
 // In-place Cartesian->spherical transform of one axis of a [OUTER][ncart(L)][INNER] array.
 template <int L, int OUTER, int INNER>
 __device__ __forceinline__ void sph_axis(double* v) {
@@ -175,14 +240,18 @@ __device__ __forceinline__ void coulomb_epilogue(const EriLaunch& a, int2 pq, co
 // of 168 registers that a third CTA needs costs at most a few spilled values, and the extra warps
 // hide more of the primitive-loop latency (measured per class on medium8 and chain20: 8-13 %
 // shorter blocks; classes further above the cap spill heavily and lose).
+// (ss|ss) keeps the 64 registers that let 8 CTAs (the shared-memory limit) share an SM.
 __host__ __device__ constexpr int eri_min_blocks(int la, int lb, int lc, int ld) {
-  return ((la == 0 && lb == 2 && lc == 0 && ld == 1) || (la == 1 && lb == 1 && lc == 0 && ld == 1) ||
-          (la == 1 && lb == 3 && lc == 0 && ld == 0))
+  return (la + lb + lc + ld == 0) ? 8
+         : ((la == 0 && lb == 2 && lc == 0 && ld == 1) ||
+            (la == 1 && lb == 1 && lc == 0 && ld == 1) || (la == 1 && lb == 3 && lc == 0 && ld == 0))
              ? 3
              : 1;
 }
 
-template <int LA, int LB, int LC, int LD, typename R>
+// ATT: the instantiation for the range-separated operators (a.potential != 0); the 1/r kernels
+// carry no attenuation code.
+template <int LA, int LB, int LC, int LD, typename R, bool ATT = false>
 __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
     eri_block(const EriLaunch a) {
   using C = gen::Cls<LA, LB, LC, LD>;
@@ -229,6 +298,8 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
         const double T = bp.zeta * rz * fma(PQx, PQx, fma(PQy, PQy, PQz * PQz));
         double F[L + 1];
         boys_eval<L>(T, s_tab, s_exp, F);
+        if constexpr (ATT)
+          boys_attenuate<L>(a.potential, a.omega, bp.zeta * rz, T, s_tab, s_exp, F);
         const double pref = bp.C * kp.C * r;
 #pragma unroll
         for (int m = 0; m <= L; ++m) F[m] *= pref;

@@ -94,6 +94,9 @@ struct EriLaunch {
   // indexed by PairDev::mol (nullptr: base / ncols above)
   const long long* mol_base;
   const long long* mol_ncols;
+  // two-electron operator: 0 = 1/r, 1 = erf(omega r)/r, 2 = erfc(omega r)/r
+  int potential;
+  double omega;
 };
 
 // Destination block of a quartet whose bra pair is P.

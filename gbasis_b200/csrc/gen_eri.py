@@ -419,6 +419,8 @@ def emit_sources(outdir, lmax):
                  "template <int LA, int LB, int LC, int LD>",
                  "int launch_t(const EriLaunch& a, int grid, cudaStream_t st) {",
                  "  if (a.fp32) eri_block<LA, LB, LC, LD, float><<<grid, kEriThreads, 0, st>>>(a);",
+                 "  else if (a.potential)",
+                 "    eri_block<LA, LB, LC, LD, double, true><<<grid, kEriThreads, 0, st>>>(a);",
                  "  else eri_block<LA, LB, LC, LD, double><<<grid, kEriThreads, 0, st>>>(a);",
                  '  return cuda_status(cudaGetLastError(), "eri class kernel launch");',
                  "}"]

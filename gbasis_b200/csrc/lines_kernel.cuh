@@ -331,7 +331,7 @@ __device__ __forceinline__ void lines_tail(const EriLaunch& a, const double* ACC
 // The kernel: per quartet, ACC[e][f] over the primitive quartets by C::prim, then the shared
 // tail (HRR, transforms, store / Schwarz / Coulomb epilogue).  Per warp shared memory:
 // ACC | W | Y | Boys values, the tail's buffers overlaying W.
-template <class C, bool COULOMB>
+template <class C, bool COULOMB, bool ATT = false>
 __global__ void __launch_bounds__(128, 4) eri_lines(const CoopArgs A) {
   extern __shared__ double smem[];
   const EriLaunch& a = A.a;
@@ -390,7 +390,8 @@ __global__ void __launch_bounds__(128, 4) eri_lines(const CoopArgs A) {
       ps.CEx = fma(ps.ze, bp.Xx, kp.Xx);
       ps.CEy = fma(ps.ze, bp.Xy, kp.Xy);
       ps.CEz = fma(ps.ze, bp.Xz, kp.Xz);
-      boys_lanes(C::L, lane, T, bp.C * kp.C * r, a.boys_tab, Fs);
+      boys_lanes(C::L, lane, T, bp.C * kp.C * r, a.boys_tab, Fs, ATT ? a.potential : 0, a.omega,
+                 bp.zeta * rz);
       __syncwarp();
       C::prim(lane, Fs, ps, W, Y, ACC, idx == 0);
       __syncwarp();
@@ -434,7 +435,8 @@ int launch_lines_t(const EriLaunch& a, const CoopMeta& m, cudaStream_t st) {
   if (s) return s;
   // the Coulomb epilogue (mode 2) is a separate instantiation, so that the store / Schwarz
   // kernel of a class with the register tail carries no interpreted tail
-  auto kern = a.mode == 2 ? eri_lines<C, true> : eri_lines<C, false>;
+  auto kern = a.potential ? (a.mode == 2 ? eri_lines<C, true, true> : eri_lines<C, false, true>)
+                          : (a.mode == 2 ? eri_lines<C, true> : eri_lines<C, false>);
   s = cuda_status(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kCoopMaxSmem), "eri_lines shared memory attribute");
   if (s) return s;
@@ -544,7 +546,7 @@ __device__ __forceinline__ void split_tail(const EriLaunch& a, double* ACC,
 // as in the light classes' kernel); the parts meet in shared memory ACC[32][NE][RS] and all
 // threads of the CTA then share the group's tail (split_tail).  Store (mode 0) and Schwarz
 // (mode 1) only.
-template <class C>
+template <class C, bool ATT = false>
 __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
   __shared__ double s_tab[kBoysNGrid * kBoysTaylor];
   __shared__ double s_exp[kBoysNGrid];
@@ -599,6 +601,8 @@ __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
           const double T = bp.zeta * rz * fma(PQx, PQx, fma(PQy, PQy, PQz * PQz));
           double F[L + 1];
           boys_eval<L>(T, s_tab, s_exp, F);
+          if constexpr (ATT)
+            boys_attenuate<L>(a.potential, a.omega, bp.zeta * rz, T, s_tab, s_exp, F);
           const double pref = bp.C * kp.C * r;
 #pragma unroll
           for (int m = 0; m <= L; ++m) F[m] *= pref;
@@ -625,14 +629,15 @@ template <class C>
 int launch_split_t(const EriLaunch& a, cudaStream_t st) {
   constexpr int NCD = ncart(C::LC) * ncart(C::LD);
   const size_t dyn = (size_t)32 * C::NE * split_rs(C::NF, NCD) * sizeof(double);
-  int s = cuda_status(cudaFuncSetAttribute(eri_split<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  auto kern = a.potential ? eri_split<C, true> : eri_split<C>;
+  int s = cuda_status(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)dyn), "eri_split shared memory attribute");
   if (s) return s;
   int dev = 0, nsm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int grid = (int)std::max<long long>(1, std::min<long long>((a.nwork + 31) / 32, (long long)nsm * (32 / C::kS)));
-  eri_split<C><<<grid, 32 * C::kS, dyn, st>>>(a);
+  kern<<<grid, 32 * C::kS, dyn, st>>>(a);
   return cuda_status(cudaGetLastError(), "eri_split launch");
 }
 

@@ -768,6 +768,8 @@ static int ensure_mixed_bounds(Basis& B, cudaStream_t st) {
 int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32) {
   int s;
   const bool mixed = skip > 0.0 || fp32 > 0.0;
+  if (mixed && B.potential)
+    return set_error(GBX_ERR_UNSUPPORTED, "the mixed-precision form computes 1/r integrals only");
   if (tau > 0.0 && (s = ensure_schwarz(B, st))) return s;
   if (mixed && (s = ensure_mixed_bounds(B, st))) return s;
   if ((s = ensure_full_work(B))) return s;
@@ -824,6 +826,8 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
     a.ncols = h.dev.ncols;
     a.mode = 0;
     a.team = h.team;
+    a.potential = B.potential;
+    a.omega = B.omega;
     const int grid =
         (int)std::max<long long>(1, std::min<long long>((h.ncand * h.team + 127) / 128, (long long)nsm * 8));
     if (per_block) cudaEventRecord(B.blk_ev[i], st);
@@ -879,6 +883,8 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
       a.nwork = len;
       a.mode = 2;
       a.team = h.team;
+      a.potential = B.potential;
+      a.omega = B.omega;
       a.D = D;
       a.J = J;
       a.nbf = B.nbf;

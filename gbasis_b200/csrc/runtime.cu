@@ -446,6 +446,18 @@ int point_charge_entry(gbx_basis* b, int npoints, const double* coords, const do
 
 extern "C" {
 
+int gbx_basis_set_potential(gbx_basis* b, int potential, double omega) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_basis_set_potential: null basis");
+  if (potential < 0 || potential > 2)
+    return set_error(GBX_ERR_INVALID, "potential must be 0 (1/r), 1 (erf) or 2 (erfc), got %d",
+                     potential);
+  if (potential != 0 && !(omega > 0.0 && omega < 1e300))
+    return set_error(GBX_ERR_INVALID, "omega must be a positive finite number for erf/erfc");
+  b->impl->potential = potential;
+  b->impl->omega = potential ? omega : 0.0;
+  return GBX_OK;
+}
+
 int gbx_release_cached_memory(void) {
   std::vector<CachedBlock> blocks;
   {

@@ -99,6 +99,10 @@ struct Basis {
   cudaEvent_t stage_ready[kStageBuffers] = {};
   cudaEvent_t stage_free[kStageBuffers] = {};
   std::vector<std::pair<void*, size_t>> dev_allocs;  // every device block the basis holds
+  // two-electron operator of the integral runs (0 = 1/r, 1 = erf(omega r)/r, 2 = erfc); the
+  // Schwarz and mixed-form bounds stay Coulomb bounds, which bound both attenuated operators
+  int potential = 0;
+  double omega = 0.0;
 
   ~Basis();
   int alloc(void** p, size_t bytes, const char* what);

@@ -65,6 +65,7 @@ class ElectronRepulsionIntegral:
     boys_func = staticmethod(_boys_host)
     _screen = 0.0
     _mixed = None  # (skip, fp32) thresholds of the mixed-precision form
+    _potential = (0, 0.0)  # two-electron operator (code, omega), see potential_code
 
     def __init__(self, contractions):
         _check_contractions(contractions)
@@ -102,6 +103,8 @@ class ElectronRepulsionIntegral:
     def _full(self, coord_types, out=None, device=None):
         db = _engine.DeviceBasis(list(self.contractions), coord_types, device=device)
         try:
+            if self._potential[0]:
+                db.set_potential(*self._potential)
             if self._mixed is None:
                 return db.full_host("chemist", self._screen, out=out)
             import ctypes
@@ -141,7 +144,7 @@ class ElectronRepulsionIntegral:
             raise TypeError("`coord_type` must be a list/tuple of the strings 'cartesian' or "
                             "'spherical'")
         return _lincomb_device(list(self.contractions), types, np.asarray(transform, dtype=float),
-                               self._screen, device)
+                               self._screen, device, self._potential)
 
 
 class ElectronRepulsionIntegralImproved(ElectronRepulsionIntegral):
@@ -152,11 +155,13 @@ class ElectronRepulsionIntegralImproved(ElectronRepulsionIntegral):
         self._screen = float(schwarz_threshold)
 
 
-def _lincomb_device(shells, types, transform, screen, device):
+def _lincomb_device(shells, types, transform, screen, device, potential=(0, 0.0)):
     import ctypes
     import torch
     db = _engine.DeviceBasis(shells, types, device=device)
     try:
+        if potential[0]:
+            db.set_potential(*potential)
         n = db.nbf
         if transform.ndim != 2 or transform.shape[1] != n:
             raise ValueError(f"`transform` must have shape (K, {n})")
@@ -191,6 +196,20 @@ def _dispatch(cls_obj, basis, transform, coord_type, out, device):
     return cls_obj.construct_array_mix(types, out=out, device=device)
 
 
+def potential_code(potential="coulomb", omega=None):
+    """Operator code of the engine for the names of gbasis's ``get_boys_function``
+    (``gbasis/integrals/boys_functions.py:283-350``): 1/r, erf(omega r)/r or erfc(omega r)/r."""
+    p = str(potential).lower()
+    if p in ["coulomb", "standard", "1/r"]:
+        return (0, 0.0)
+    if p in ["erf", "erf_coulomb", "erfc", "erfc_coulomb"]:
+        kind = "erf" if p.startswith("erf_") or p == "erf" else "erfc"
+        if omega is None:
+            raise ValueError(f"omega parameter is required for {kind}-attenuated potential")
+        return (1 if kind == "erf" else 2, float(omega))
+    raise ValueError(f"Unknown potential type: {potential}. Valid options: coulomb, erf, erfc")
+
+
 # Mixed form thresholds on B_pq = Q_p Q_q, Q_p = sqrt(max |(ab|ab)|) over the pair's output
 # functions (a rigorous bound on |(ab|cd)|).  Skipped quartets contribute at most MIXED_SKIP;
 # the FP32 recursions lose up to ~1e-4 of B_pq on f-containing classes (measured: 20-atom
@@ -202,18 +221,22 @@ MIXED_FP32 = 2e-7
 
 def electron_repulsion_integral(basis, transform=None, notation="physicist", *, coord_type=None,
                                 device=None, out=None, precision="fp64", mixed_skip=MIXED_SKIP,
-                                mixed_fp32=MIXED_FP32):
+                                mixed_fp32=MIXED_FP32, potential="coulomb", omega=None):
     """ERIs of ``basis`` (``electron_repulsion.py:214-281``): (K, K, K, K) float64, physicist
     notation by default (a ``transpose(0, 2, 1, 3)`` view of the chemist array).
 
     ``precision="mixed"`` selects the mixed form: quartets whose final-value Schwarz bound is
     below ``mixed_skip`` are zero, those below ``mixed_fp32`` run their vertical and transfer
-    recursions in FP32."""
+    recursions in FP32.  ``potential`` ("coulomb", "erf" or "erfc", with ``omega``) selects the
+    operator, as ``get_boys_function`` does for the reference's integral classes."""
     if notation not in ["physicist", "chemist"]:
         raise ValueError("`notation` must be one of 'physicist' or 'chemist'")
     if precision not in ("fp64", "mixed"):
         raise ValueError("`precision` must be 'fp64' or 'mixed'")
     obj = ElectronRepulsionIntegral(basis)
+    obj._potential = potential_code(potential, omega)
+    if precision == "mixed" and obj._potential[0]:
+        raise NotImplementedError("the mixed-precision form computes 1/r integrals only")
     if precision == "mixed":
         obj._mixed = (float(mixed_skip), float(mixed_fp32))
     array = _dispatch(obj, basis, transform, coord_type, out, device)
@@ -224,13 +247,14 @@ def electron_repulsion_integral(basis, transform=None, notation="physicist", *, 
 
 def electron_repulsion_integral_improved(basis, transform=None, notation="physicist",
                                          schwarz_threshold=0.0, *, coord_type=None, device=None,
-                                         out=None):
+                                         out=None, potential="coulomb", omega=None):
     """``electron_repulsion.py:415-504``: as :func:`electron_repulsion_integral`, with shell
     quartets whose Schwarz bound Q_ij Q_kl (blocks without ``norm_cont``) is below
-    ``schwarz_threshold`` set to zero."""
+    ``schwarz_threshold`` set to zero (Coulomb bounds, also for the erf/erfc operators)."""
     if notation not in ["physicist", "chemist"]:
         raise ValueError("`notation` must be one of 'physicist' or 'chemist'")
     obj = ElectronRepulsionIntegralImproved(basis, schwarz_threshold)
+    obj._potential = potential_code(potential, omega)
     array = _dispatch(obj, basis, transform, coord_type, out, device)
     if notation == "physicist":
         array = np.transpose(array, (0, 2, 1, 3))

@@ -73,6 +73,14 @@ int gbx_basis_create(gbx_basis** out, int n_shells, const int* angmom, const int
                      const int* nout, const int* sph, const int8_t* pos, const double* scl,
                      int device);
 int gbx_basis_destroy(gbx_basis* b);
+
+/* Two-electron operator of the basis's later integral calls (full tensor, unique integrals, J,
+ * J/K): 0 = 1/r, 1 = erf(omega r)/r (long range), 2 = erfc(omega r)/r (short range), the
+ * range-separated operators of gbasis/integrals/boys_functions.py:145-223 and
+ * get_boys_function (:283-350) that ElectronRepulsionIntegralImproved takes as its boys_func
+ * (gbasis/integrals/electron_repulsion.py:284-303).  Schwarz screening keeps the Coulomb
+ * bounds, which also bound both attenuated operators (as the reference's screener does). */
+int gbx_basis_set_potential(gbx_basis* b, int potential, double omega);
 /* Original (generalized-contraction) shell of each segmented shell: Schwarz bounds of a
  * quartet use the bound of the original shell pairs, as gbasis screens whole generalized
  * shells.  Default: every segmented shell is its own group. */

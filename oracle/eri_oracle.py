@@ -212,12 +212,15 @@ def _first_dir(t):
     raise ValueError
 
 
-def quartet_cartesian(sa, sb, sc, sd):
+def quartet_cartesian(sa, sb, sc, sd, potential=(0, 0.0)):
     """Contracted Cartesian block (L_a, L_b, L_c, L_d, M_a, M_b, M_c, M_d).
 
     Mirrors the output of ``_compute_two_elec_integrals`` (``_two_elec_int.py:149-814``):
     primitive and Cartesian-component normalisation applied, ``norm_cont`` not applied,
-    component order taken from each shell's ``angmom_components_cart``.
+    component order taken from each shell's ``angmom_components_cart``.  ``potential`` = (1,
+    omega) or (2, omega) selects erf(omega r)/r or erfc(omega r)/r through the modified Boys
+    values of ``boys_functions.py:145-223`` (the ``boys_func(orders, T, rho=...)`` call of
+    ``_two_elec_int_improved.py:697``).
     """
     la, lb, lc, ld = sa.angmom, sb.angmom, sc.angmom, sd.angmom
     L = la + lb + lc + ld
@@ -236,6 +239,12 @@ def quartet_cartesian(sa, sb, sc, sd):
     kcd = np.exp(-c * d / eta * np.dot(CD, CD))
     pref = 2.0 * np.pi ** 2.5 / (zeta * eta * np.sqrt(zeta + eta)) * kab * kcd
     F = boys(np.arange(L + 1)[:, None], T[None, :])  # (L+1, nprim)
+    if potential[0]:
+        w2 = float(potential[1]) ** 2
+        att = w2 / (w2 + rho)
+        Fa = att[None, :] ** (np.arange(L + 1)[:, None] + 0.5) * boys(np.arange(L + 1)[:, None],
+                                                                     (att * T)[None, :])
+        F = Fa if potential[0] == 1 else F - Fa
     WP = -(rho / zeta)[:, None] * PQ
     r_z = rho / zeta
     o2z = 0.5 / zeta
@@ -330,7 +339,7 @@ def quartet_cartesian(sa, sb, sc, sd):
     return out
 
 
-def construct_array_contraction(sa, sb, sc, sd, reorder=False):
+def construct_array_contraction(sa, sb, sc, sd, reorder=False, potential=(0, 0.0)):
     """(M1, L1, M2, L2, M3, L3, M4, L4), chemist (``electron_repulsion.py:86-211``).
 
     ``reorder=True`` first swaps shells so that l_a >= l_b, l_c >= l_d and l_a >= l_c and
@@ -339,9 +348,9 @@ def construct_array_contraction(sa, sb, sc, sd, reorder=False):
     higher-l centres, which loses far fewer digits for diffuse high-l quartets.
     """
     if not reorder:
-        return np.transpose(quartet_cartesian(sa, sb, sc, sd), (4, 0, 5, 1, 6, 2, 7, 3))
+        return np.transpose(quartet_cartesian(sa, sb, sc, sd, potential), (4, 0, 5, 1, 6, 2, 7, 3))
     if reorder == "exponent":
-        return _exponent_oriented(sa, sb, sc, sd)
+        return _exponent_oriented(sa, sb, sc, sd, potential)
     bra_sw = sa.angmom < sb.angmom
     if bra_sw:
         sa, sb = sb, sa
@@ -351,7 +360,7 @@ def construct_array_contraction(sa, sb, sc, sd, reorder=False):
     bk_sw = sa.angmom < sc.angmom
     if bk_sw:
         sa, sb, sc, sd = sc, sd, sa, sb
-    x = quartet_cartesian(sa, sb, sc, sd)  # (La, Lb, Lc, Ld, Ma, Mb, Mc, Md)
+    x = quartet_cartesian(sa, sb, sc, sd, potential)  # (La, Lb, Lc, Ld, Ma, Mb, Mc, Md)
     if bk_sw:
         x = np.transpose(x, (2, 3, 0, 1, 6, 7, 4, 5))
     if ket_sw:
@@ -365,7 +374,7 @@ def _pair_key(a, b):
     return (a + b, max(a, b), a)
 
 
-def _exponent_oriented(sa, sb, sc, sd):
+def _exponent_oriented(sa, sb, sc, sd, potential=(0, 0.0)):
     """Same integrals with the recursions run from the shell of larger maximum exponent of
     each pair and the bra being the pair of larger (l_a + l_b, max l, l_a) — the recursion
     order of the B200 engine (``gbasis_b200/csrc/runtime.cu``)."""
@@ -384,7 +393,7 @@ def _exponent_oriented(sa, sb, sc, sd):
     if _pair_key(s[2].angmom, s[3].angmom) > _pair_key(s[0].angmom, s[1].angmom):
         s = s[2:] + s[:2]
         perm = perm[2:] + perm[:2]
-    x = quartet_cartesian(*s)  # axes in the order of s
+    x = quartet_cartesian(*s, potential)  # axes in the order of s
     inv = list(np.argsort(perm))
     x = np.transpose(x, inv + [4 + v for v in inv])
     return np.transpose(x, (4, 0, 5, 1, 6, 2, 7, 3))
@@ -409,7 +418,8 @@ def _shell_matrix(shell, ctype):
     return W
 
 
-def construct_array(basis, coord_types, quartet_fn=None, screen=None, reorder=False):
+def construct_array(basis, coord_types, quartet_fn=None, screen=None, reorder=False,
+                    potential=(0, 0.0)):
     """Full 4-index array in chemist order for per-shell coordinate types.
 
     Restates ``construct_array_cartesian/spherical/mix`` (``base_four_symm.py:160-557``):
@@ -419,7 +429,8 @@ def construct_array(basis, coord_types, quartet_fn=None, screen=None, reorder=Fa
     (the improved path, ``electron_repulsion.py:341-361``).
     """
     if quartet_fn is None:
-        quartet_fn = lambda a, b, c, d: construct_array_contraction(a, b, c, d, reorder)  # noqa: E731
+        quartet_fn = lambda a, b, c, d: construct_array_contraction(a, b, c, d, reorder,  # noqa: E731
+                                                                    potential)
     Ws = [_shell_matrix(s, t) for s, t in zip(basis, coord_types)]
     sizes = [W.shape[0] for W in Ws]
     off = np.concatenate([[0], np.cumsum(sizes)]).astype(int)
@@ -461,11 +472,12 @@ def _coord_types(basis):
     return out
 
 
-def electron_repulsion_integral(basis, transform=None, notation="physicist", reorder=False):
+def electron_repulsion_integral(basis, transform=None, notation="physicist", reorder=False,
+                                potential=(0, 0.0)):
     """``electron_repulsion.py:214-281``: dispatch, then physicist = transpose(0,2,1,3)."""
     if notation not in ("physicist", "chemist"):
         raise ValueError("`notation` must be one of 'physicist' or 'chemist'")
-    arr = construct_array(list(basis), _coord_types(basis), reorder=reorder)
+    arr = construct_array(list(basis), _coord_types(basis), reorder=reorder, potential=potential)
     if transform is not None:
         arr = construct_array_lincomb(arr, transform)
     if notation == "physicist":
