@@ -1,0 +1,41 @@
+"""Host-side argument handling of the added entry points (no GPU needed: every case raises
+before a device is touched)."""
+import numpy as np
+import pytest
+
+from conftest import load_npz, shells_from_json
+from gbasis_b200 import point_charge as pc
+from gbasis_b200.electron_repulsion import potential_code
+
+
+def test_potential_names_follow_get_boys_function():
+    # gbasis/integrals/boys_functions.py:283-350
+    for name in ("coulomb", "standard", "1/r", "Coulomb"):
+        assert potential_code(name) == (0, 0.0)
+    assert potential_code("erf", 0.4) == (1, 0.4)
+    assert potential_code("erf_coulomb", 0.4) == (1, 0.4)
+    assert potential_code("erfc", 1.5) == (2, 1.5)
+    assert potential_code("ERFC_COULOMB", 1.5) == (2, 1.5)
+    with pytest.raises(ValueError, match="omega parameter is required for erf-attenuated"):
+        potential_code("erf")
+    with pytest.raises(ValueError, match="omega parameter is required for erfc-attenuated"):
+        potential_code("erfc")
+    with pytest.raises(ValueError, match="Unknown potential type"):
+        potential_code("yukawa", 1.0)
+
+
+def test_point_charge_argument_checks():
+    # gbasis/integrals/point_charge.py:180-218
+    basis = shells_from_json(load_npz("tiny4.npz")["shells"])
+    with pytest.raises(TypeError):
+        pc.point_charge_integral(basis, [[0.0, 0.0, 0.0]], np.ones(1))
+    with pytest.raises(TypeError):
+        pc.point_charge_integral(basis, np.zeros((2, 2)), np.ones(2))
+    with pytest.raises(TypeError):
+        pc.point_charge_integral(basis, np.zeros((2, 3)), np.ones((2, 1)))
+    with pytest.raises(TypeError):
+        pc.point_charge_integral(basis, np.zeros((2, 3), dtype=complex), np.ones(2))
+    with pytest.raises(ValueError):
+        pc.nuclear_electron_attraction_integral(basis, np.zeros((2, 3)), np.ones(3))
+    with pytest.raises(TypeError):
+        pc.point_charge_integral([object()], np.zeros((1, 3)), np.ones(1))
