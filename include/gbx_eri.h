@@ -224,7 +224,8 @@ int gbx_block_times(gbx_basis* b, double* ms, int n);
  * nuclear_electron_attraction_integral, gbasis/integrals/nuclear_electron_attraction.py:8-42):
  *   sum_points = 0: out[(a*N + b)*n_points + c] = -charges[c] (a| 1/|r - R_c| |b)
  *   sum_points = 1: out[a*N + b] = sum_c -charges[c] (a| 1/|r - R_c| |b)
- * coords: host n_points x 3, charges: host n_points (finite); out: device, row-major. */
+ * coords: host n_points x 3, charges: host n_points (finite); out: device, row-major.  The call
+ * returns once the kernels are done (it synchronizes `stream`). */
 int gbx_point_charge(gbx_basis* b, int n_points, const double* coords, const double* charges,
                      int sum_points, double* out, void* stream);
 
