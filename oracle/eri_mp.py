@@ -4,7 +4,7 @@ Evaluates the same Obara-Saika / electron-transfer / horizontal recursions as
 :mod:`oracle.eri_oracle` (which follows ``gbasis/integrals/_two_elec_int.py:149-814``)
 on scalars in mpmath with 40 significant digits.  Every recursion path then gives
 the same value to far below double precision, so this is the "true" value a double
-implementation is judged against where the double-precision reference itself loses
+implementation is measured against where the double-precision reference itself loses
 digits (diffuse high-l quartets, where gbasis's two ERI paths disagree with each other).
 """
 from __future__ import annotations
