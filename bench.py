@@ -41,7 +41,7 @@ UNIT = "ERI/s"
 EXPAND_TRAFFIC_BYTES = 404.778752e6 + 1599.436e6
 
 
-HBM_FALLBACK_GBS = 6650.0  # copy bandwidth measured earlier on this pool's B200s
+HBM_FALLBACK_GBS = 6650.0  # copy bandwidth measured earlier on a B200 of the same kind
 
 
 def _peaks():
@@ -117,6 +117,23 @@ class ClockSampler:
         sm = self.samples
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.max_mhz,
                 "reasons": sorted(self.reasons), "samples": len(sm), "source": "NVML"}
+
+
+def max_over_ranks(x, dist, device):
+    """The largest of every rank's ``x`` (a time); every rank of the group must call it, in the
+    same order.  ``dist`` is ``torch.distributed`` or None for a single process."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, units_per_rank, ms):
+    """Whole-job units per second of ``world`` independent replicas, each processing
+    ``units_per_rank`` units, timed by the slowest rank (``ms`` per step)."""
+    return world * units_per_rank / (ms * 1e-3)
 
 
 def cpu_baseline(shells, seconds=12.0, seed=0):
@@ -357,12 +374,8 @@ def main():
             step()
         e1.record(stream)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / a.steps
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * n_unique / (ms * 1e-3)
+    ms = max_over_ranks(e0.elapsed_time(e1) / a.steps, dist, dev)
+    value = replica_throughput(world, n_unique, ms)
 
     # mixed-precision form on the same workload, and its error against the FP64 tensor
     from gbasis_b200.electron_repulsion import MIXED_FP32, MIXED_SKIP
@@ -401,7 +414,7 @@ def main():
     hbm = peaks.get("hbm_gbs")
     hbm_source = "MEASURED_PEAKS.json hbm_gbs (of measured)"
     if not hbm:
-        # no measured copy bandwidth on this machine: the pool's earlier measurement
+        # no measured copy bandwidth on this machine: the earlier B200 measurement
         hbm, hbm_source = HBM_FALLBACK_GBS, "fallback 6650 GB/s copy bandwidth (of fallback)"
     compute_tf = flops / (ph[1] * 1e-3) / 1e12
     exp_bytes = 8.0 * n ** 4 + compact_bytes  # tensor written + compact store read once
@@ -428,7 +441,7 @@ def main():
     t0 = time.perf_counter()
     for _ in range(a.e2e_steps):
         res = er.electron_repulsion_integral(shells, out=pinned)
-    e2e_s = (time.perf_counter() - t0) / a.e2e_steps
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / a.e2e_steps, dist, dev)
     assert res.shape == (n, n, n, n)
     # floor of the host-output path on this machine: one plain device-to-host copy of the
     # tensor's bytes into the same page-locked buffer
@@ -440,7 +453,8 @@ def main():
     host.copy_(src, non_blocking=True)
     torch.cuda.synchronize()
     d2h_s = time.perf_counter() - t1
-    e2e = {"value": world * n_unique / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+    e2e = {"value": replica_throughput(world, n_unique, e2e_s * 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": 8 * n ** 4, "ms_per_step": e2e_s * 1e3,
            "d2h_copy_floor_ms": d2h_s * 1e3,
            "d2h_copy_gbs": 8 * n ** 4 / d2h_s / 1e9}
