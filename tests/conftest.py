@@ -76,3 +76,18 @@ def expand_unique(n, values):
 @pytest.fixture(scope="session")
 def golden():
     return load_npz
+
+
+def horton_overflow_case():
+    """Shells, component indices and values of the large-exponent (ss|ff) known answer
+    (``horton_overflow.json``, from gbasis ``tests/test_two_elec_int.py``)."""
+    rec = json.load(open(os.path.join(GOLDEN, "horton_overflow.json")))
+    shells, idx = [], []
+    for s in rec["shells"]:
+        g = GeneralizedContractionShell(int(s["angmom"]), np.array(s["coord"], dtype=float),
+                                        np.array(s["coeffs"], dtype=float),
+                                        np.array(s["exps"], dtype=float), "cartesian")
+        comps = [tuple(int(v) for v in row) for row in g.angmom_components_cart]
+        idx.append(comps.index(tuple(s["components"][0])))
+        shells.append(g)
+    return shells, idx, rec

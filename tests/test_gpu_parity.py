@@ -208,3 +208,21 @@ def test_errors_match_reference_behaviour():
         er.ElectronRepulsionIntegral([])
     with pytest.raises(ValueError):
         er.ElectronRepulsionIntegral(shells).construct_array_mix(["cartesian"])
+
+
+def test_horton_large_exponent_quartet():
+    """gbasis tests/test_two_elec_int.py ``test_compute_two_elec_integrals_overflow_horton``,
+    an xfail in the reference (its double path loses every digit of this (ss|ff) quartet):
+    the engine runs the recursions from the f pair and matches the 40-digit value and HORTON's
+    value, in both pair orders."""
+    from conftest import horton_overflow_case
+    shells, i, rec = horton_overflow_case()
+    truth = rec["truth_40_digits"]
+    blk = er.ElectronRepulsionIntegral.construct_array_contraction(*shells)
+    assert blk.shape == (1, 1, 1, 1, 1, 10, 1, 10)
+    got = blk[0, i[0], 0, i[1], 0, i[2], 0, i[3]]
+    assert abs(got - truth) <= ATOL
+    assert np.allclose(got, rec["horton"])  # the reference test's tolerance
+    blk = er.ElectronRepulsionIntegral.construct_array_contraction(shells[2], shells[3],
+                                                                   shells[0], shells[1])
+    assert abs(blk[0, i[2], 0, i[3], 0, i[0], 0, i[1]] - truth) <= ATOL

@@ -135,3 +135,24 @@ def test_mixed_basis(kind):
         assert np.max(np.abs(got - ref)) <= max(ATOL, 8 * ref_err)
         if reorder:
             assert np.max(np.abs(got - truth)) <= max(ATOL, 4 * ref_err)
+
+
+def test_horton_large_exponent_quartet():
+    """gbasis tests/test_two_elec_int.py ``test_compute_two_elec_integrals_overflow_horton``
+    (xfail in the reference): an (ss|ff) quartet of tightly contracted, alternating-sign s
+    shells.  The reference's double path, which transfers angular momentum from the s pair,
+    misses HORTON's value entirely; the 40-digit evaluator reproduces it, and so does the
+    oracle in the recursion order of the engine (the f pair as the bra, no transfer)."""
+    from conftest import horton_overflow_case
+    shells, i, rec = horton_overflow_case()
+    truth, horton = rec["truth_40_digits"], rec["horton"]
+    # HORTON's value to the reference test's own tolerance (np.allclose defaults)
+    assert np.allclose(truth, horton)
+    assert abs(rec["reference_double"] - horton) > 1e-3  # the reference's known failure
+    blk = orc.construct_array_contraction(*shells, reorder="exponent")
+    got = blk[0, i[0], 0, i[1], 0, i[2], 0, i[3]]
+    assert abs(got - truth) <= ATOL
+    # the same integral with the pairs exchanged, (ff|ss)
+    blk = orc.construct_array_contraction(shells[2], shells[3], shells[0], shells[1],
+                                          reorder="exponent")
+    assert abs(blk[0, i[2], 0, i[3], 0, i[0], 0, i[1]] - truth) <= ATOL
