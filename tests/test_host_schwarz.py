@@ -1,0 +1,52 @@
+"""Schwarz screening interface on the CPU: primitive pair screening and argument checks of
+``gbasis_b200.schwarz_screening`` (no device call), and the oracle's bounds pinned to the
+reference's own ``SchwarzScreener`` bounds (``schwarz.npz``, written from gbasis by
+``tests/golden/make_schwarz_golden.py``)."""
+import numpy as np
+import pytest
+
+from conftest import load_npz, shells_from_json
+from gbasis_b200 import schwarz_screening as sz
+from gbasis_b200.contractions import GeneralizedContractionShell
+from oracle import eri_oracle as orc
+
+
+def _fixture():
+    z = load_npz("schwarz.npz")
+    return z, shells_from_json(z["shells"])
+
+
+def test_shell_pair_significant_matches_reference():
+    # gbasis/integrals/_schwarz_screening.py:93-128
+    z, shells = _fixture()
+    for t in z["thresholds"]:
+        got = [sz.shell_pair_significant(shells[i], shells[j], t) for i, j in z["pairs"]]
+        np.testing.assert_array_equal(got, z[f"pair_{t:g}"])
+
+
+def test_shell_pair_significant_cases():
+    # the cases of gbasis tests/test_schwarz_screening.py:79-118
+    def s(c, e):
+        return GeneralizedContractionShell(0, np.array(c, dtype=float), np.array([1.0]),
+                                           np.array([e]), "cartesian")
+    assert sz.shell_pair_significant(s([0, 0, 0], 1.0), s([0, 0, 0], 1.0))
+    assert sz.shell_pair_significant(s([0, 0, 0], 1.0), s([1, 0, 0], 1.0))
+    assert not sz.shell_pair_significant(s([0, 0, 0], 10.0), s([50, 0, 0], 10.0))
+    assert sz.shell_pair_significant(s([0, 0, 0], 0.01), s([5, 0, 0], 0.01))
+    a, b = s([0, 0, 0], 1.0), s([3, 0, 0], 1.0)  # decay exp(-4.5) = 1.1e-2
+    assert sz.shell_pair_significant(a, b, threshold=1e-3)
+    assert not sz.shell_pair_significant(a, b, threshold=0.1)
+
+
+def test_oracle_bounds_match_reference():
+    z, shells = _fixture()
+    np.testing.assert_allclose(orc.schwarz_bounds(shells), z["bounds"], rtol=1e-10, atol=1e-14)
+
+
+def test_argument_checks():
+    with pytest.raises(TypeError):
+        sz.compute_schwarz_bounds("not a list")
+    with pytest.raises(ValueError):
+        sz.compute_schwarz_bounds([])
+    with pytest.raises(TypeError):
+        sz.SchwarzScreener([object()])
