@@ -33,7 +33,7 @@ EXPORTED_SYMBOLS = (
     "gbx_batch_set_graph", "gbx_unique_values", "gbx_compact_view",
     "gbx_batch_num_types", "gbx_batch_type_info", "gbx_batch_set_team", "gbx_batch_set_profiling",
     "gbx_batch_type_times", "gbx_release_cached_memory", "gbx_eri_jk", "gbx_point_charge",
-    "gbx_basis_set_potential",
+    "gbx_basis_set_potential", "gbx_batch_run_mixed", "gbx_batch_mixed_counts",
 )
 
 
@@ -106,6 +106,9 @@ def lib():
             "gbx_eri_jk": [_P, _P, _D, _P, _P, _P],
             "gbx_point_charge": [_P, _I, _P, _P, _I, _P, _P],
             "gbx_basis_set_potential": [_P, _I, _D],
+            "gbx_batch_run_mixed": [_P, _I, _D, _D, _P, _P],
+            "gbx_batch_mixed_counts": [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64),
+                                       ctypes.POINTER(_I64)],
         }
         for name, args in sig.items():
             f = getattr(L, name)

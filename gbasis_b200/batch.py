@@ -113,9 +113,13 @@ class EriBatch:
                 json.dump(table, f, indent=1, sort_keys=True)
         return chosen, times
 
-    def run(self, outs, notation="chemist", stream=None):
+    def run(self, outs, notation="chemist", stream=None, mixed=None):
         """Write molecule m's (N_m,)*4 float64 tensor to device buffer ``outs[m]`` (torch
-        tensors or raw device pointers).  Asynchronous on ``stream``."""
+        tensors or raw device pointers).  Asynchronous on ``stream``.
+
+        ``mixed=(skip, fp32)`` runs the mixed-precision form: quartets whose final-value bound
+        is below ``skip`` are zero, those below ``fp32`` (light classes) run their recursions
+        in FP32.  Its first run computes the batch's bounds (synchronously)."""
         if notation not in ("physicist", "chemist"):
             raise ValueError("`notation` must be one of 'physicist' or 'chemist'")
         if len(outs) != self.n_mol:
@@ -130,8 +134,20 @@ class EriBatch:
             else:
                 ptrs[m] = int(o)
         code = _engine.GBX_PHYSICIST if notation == "physicist" else _engine.GBX_CHEMIST
-        _engine.check(_engine.lib().gbx_batch_run(self.handle, code, ptrs, stream),
-                      "gbx_batch_run")
+        if mixed is None:
+            _engine.check(_engine.lib().gbx_batch_run(self.handle, code, ptrs, stream),
+                          "gbx_batch_run")
+        else:
+            _engine.check(_engine.lib().gbx_batch_run_mixed(
+                self.handle, code, float(mixed[0]), float(mixed[1]), ptrs, stream),
+                "gbx_batch_run_mixed")
+
+    def mixed_counts(self):
+        """(FP64, FP32, left-out) quartets of the last mixed-form lists."""
+        v = [ctypes.c_int64() for _ in range(3)]
+        _engine.check(_engine.lib().gbx_batch_mixed_counts(self.handle, *map(ctypes.byref, v)),
+                      "gbx_batch_mixed_counts")
+        return tuple(int(x.value) for x in v)
 
     def close(self):
         if getattr(self, "handle", None):
@@ -145,17 +161,27 @@ class EriBatch:
             pass
 
 
-def electron_repulsion_integral_batch(molecules, notation="physicist", device=None):
+def electron_repulsion_integral_batch(molecules, notation="physicist", device=None,
+                                      precision="fp64", mixed_skip=None, mixed_fp32=None):
     """ERI tensors of every molecule as device-resident torch tensors of shape (N_m,)*4;
     ``notation`` as in ``electron_repulsion_integral`` (physicist is the
-    ``permute(0, 2, 1, 3)`` view of the chemist tensor)."""
+    ``permute(0, 2, 1, 3)`` view of the chemist tensor).  ``precision="mixed"`` selects the
+    mixed form with the thresholds of ``electron_repulsion_integral``."""
     import torch
+    from .electron_repulsion import MIXED_FP32, MIXED_SKIP
     if notation not in ["physicist", "chemist"]:
         raise ValueError("`notation` must be one of 'physicist' or 'chemist'")
+    if precision not in ("fp64", "mixed"):
+        raise ValueError("`precision` must be 'fp64' or 'mixed'")
+    mixed = None
+    if precision == "mixed":
+        mixed = (MIXED_SKIP if mixed_skip is None else float(mixed_skip),
+                 MIXED_FP32 if mixed_fp32 is None else float(mixed_fp32))
     b = EriBatch(molecules, device=device)
     dev = torch.device("cuda", b.device)
     outs = [torch.empty((n,) * 4, dtype=torch.float64, device=dev) for n in b.nbf]
-    b.run(outs, "chemist", stream=ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    b.run(outs, "chemist", stream=ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream),
+          mixed=mixed)
     torch.cuda.current_stream(dev).synchronize()
     b.close()
     if notation == "physicist":

@@ -18,6 +18,7 @@
 #include "gbx_eri.h"
 #include "gbx_common.cuh"
 #include "pipeline_kernels.cuh"
+#include "coop.cuh"
 #include "runtime.h"
 
 namespace gbx {
@@ -72,6 +73,18 @@ struct Batch {
   bool profile = false;
   std::vector<cudaEvent_t> type_ev;
   std::vector<void*> allocs;
+  // mixed-precision form: the FP64 work list and first merged pair of each molecule kept on
+  // the host; per pair the bound of its output functions; per type, in d_work_mixed, the
+  // FP64 quartets followed by the FP32 ones (quartets below the skip bound left out)
+  std::vector<int2> h_work;
+  std::vector<long long> pair_off;
+  std::vector<double> h_qmixed;
+  int2* d_work_mixed = nullptr;
+  std::vector<long long> mix_off, mix_n64, mix_n32;
+  long long mix_count[3] = {0, 0, 0};  // FP64, FP32, skipped quartets
+  double mix_skip = -1.0, mix_fp32 = -1.0;
+  cudaGraph_t graph_m = nullptr;
+  cudaGraphExec_t graph_exec_m = nullptr;
 
   int alloc(void** p, size_t bytes, const char* what) {
     if (bytes == 0) bytes = 16;
@@ -92,6 +105,8 @@ struct Batch {
     cudaSetDevice(device);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
+    if (graph_exec_m) cudaGraphExecDestroy(graph_exec_m);
+    if (graph_m) cudaGraphDestroy(graph_m);
     for (void* p : allocs) cudaFree(p);
     for (cudaStream_t s : aux) cudaStreamDestroy(s);
     for (cudaEvent_t e : join) cudaEventDestroy(e);
@@ -221,6 +236,8 @@ static int build_batch(Batch& Bt, int n_mol, const int* mol_nshells, const int* 
   if ((s = Bt.upload(&Bt.d_exps, hexps, "upload batch exponents"))) return s;
   if ((s = Bt.upload(&Bt.d_coefs, hcoefs, "upload batch coefficients"))) return s;
   if ((s = Bt.upload(&Bt.d_work, work, "upload batch work list"))) return s;
+  Bt.h_work = std::move(work);
+  Bt.pair_off = pair_off;
   if ((s = Bt.alloc((void**)&Bt.d_prims, (size_t)std::max<long long>(pp0, 1) * sizeof(PrimPair),
                     "cudaMalloc(batch primitive pairs)")))
     return s;
@@ -293,13 +310,161 @@ static int build_batch(Batch& Bt, int n_mol, const int* mol_nshells, const int* 
   return GBX_OK;
 }
 
-// The launches of one batch run on stream `st` (class kernels on the auxiliary streams).
-static int enqueue_batch(Batch& Bt, cudaStream_t st) {
+// Mixed form, bounds: Q_p = sqrt(max |(ab|ab)|) over the output functions of every merged
+// pair, as a single basis computes them (Cauchy-Schwarz for the final values, so
+// |(ab|cd)| <= Q_p Q_q).  The diagonal quartets (p, p) of all molecules run through the class
+// kernels into the batch compact store (scratch here: every run overwrites it), then
+// diagonal_bounds reads each molecule's diagonals.  Once per batch, on Bt.exec, synchronous.
+static int batch_mixed_bounds(Batch& Bt) {
+  if (!Bt.h_qmixed.empty()) return GBX_OK;
+  const long long np = Bt.pair_off[Bt.nmol];
+  std::vector<int2> diag;
+  diag.reserve((size_t)np);
+  std::vector<long long> first(kNumPairClasses + 1, 0);
+  for (int c = 0; c < kNumPairClasses; ++c) {
+    first[c] = (long long)diag.size();
+    for (int m = 0; m < Bt.nmol; ++m) {
+      const Basis& B = *Bt.mols[m];
+      for (long long pl = 0; pl < B.class_count[c]; ++pl) {
+        const int p = (int)(Bt.pair_off[m] + B.class_first[c] + pl);
+        diag.push_back(make_int2(p, p));
+      }
+    }
+  }
+  first[kNumPairClasses] = (long long)diag.size();
+  if ((long long)diag.size() != np)
+    return set_error(GBX_ERR_INVALID, "batch pair classes cover %lld of %lld pairs",
+                     (long long)diag.size(), np);
+  int2* d_diag = nullptr;
+  double* d_q = nullptr;
+  GBX_CUDA(cudaMalloc(&d_diag, std::max<size_t>(diag.size(), 1) * sizeof(int2)),
+           "cudaMalloc(batch diagonal quartets)");
+  cudaError_t e = cudaMalloc(&d_q, std::max<long long>(np, 1) * sizeof(double));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(d_diag, diag.data(), diag.size() * sizeof(int2), cudaMemcpyHostToDevice);
+  int s = cuda_status(e, "batch mixed-form bounds setup");
   const int nsm = num_sms_of(Bt.device);
+  for (int c = 0; c < kNumPairClasses && !s; ++c) {
+    const long long n = first[c + 1] - first[c];
+    if (n == 0) continue;
+    const BatchType* T = nullptr;
+    for (const BatchType& t : Bt.types)
+      if (t.cb == c && t.ck == c) T = &t;
+    if (!T) {
+      s = set_error(GBX_ERR_INVALID, "batch has pairs of class %d but no diagonal block type", c);
+      break;
+    }
+    EriLaunch a;
+    memset(&a, 0, sizeof(a));
+    a.pairs = Bt.d_pairs;
+    a.prims = Bt.d_prims;
+    a.shells = Bt.d_shells;
+    a.boys_tab = Bt.d_boys;
+    a.out = Bt.d_compact;
+    a.work = d_diag;
+    a.work_off = first[c];
+    a.nwork = n;
+    a.mode = 0;
+    a.team = 1;
+    a.mol_base = T->d_base;
+    a.mol_ncols = T->d_ncols;
+    const int grid = (int)std::max<long long>(1, std::min<long long>((n + 127) / 128,
+                                                                     (long long)nsm * 8));
+    s = launch_class(kPairClassL[c][0], kPairClassL[c][1], kPairClassL[c][0], kPairClassL[c][1],
+                     a, grid, Bt.exec);
+  }
+  for (int m = 0; m < Bt.nmol && !s; ++m)
+    s = launch_diagonal_bounds(Bt.d_pairs + Bt.pair_off[m],
+                               (int)(Bt.pair_off[m + 1] - Bt.pair_off[m]), Bt.d_shells,
+                               Bt.h_exp[m].blocks, Bt.h_exp[m].compact, d_q + Bt.pair_off[m],
+                               Bt.exec);
+  e = cudaStreamSynchronize(Bt.exec);
+  if (!s) s = cuda_status(e, "batch mixed-form bounds");
+  if (!s) {
+    Bt.h_qmixed.resize((size_t)np);
+    s = cuda_status(cudaMemcpy(Bt.h_qmixed.data(), d_q, np * sizeof(double),
+                               cudaMemcpyDeviceToHost), "download batch bounds");
+    if (s) Bt.h_qmixed.clear();
+  }
+  cudaFree(d_diag);
+  if (d_q) cudaFree(d_q);
+  return s;
+}
+
+// Drops the captured graph of the mixed form (thresholds or teams changed).
+static void batch_drop_mixed_graph(Batch& B) {
+  if (B.graph_exec_m) cudaGraphExecDestroy(B.graph_exec_m);
+  if (B.graph_m) cudaGraphDestroy(B.graph_m);
+  B.graph_exec_m = nullptr;
+  B.graph_m = nullptr;
+}
+
+// Mixed form, work lists: per block type the FP64 quartets, then those whose bound is below
+// `fp32` (light classes only: the register kernel has the FP32 recursions), leaving out those
+// below `skip`.  The thresholds decide exactly as the single-basis work-list build does.
+static int batch_mixed_lists(Batch& Bt, double skip, double fp32) {
+  if (Bt.d_work_mixed && skip == Bt.mix_skip && fp32 == Bt.mix_fp32) return GBX_OK;
+  int s;
+  if ((s = batch_mixed_bounds(Bt))) return s;
+  const size_t nt = Bt.types.size();
+  std::vector<int2> w, w32;
+  w.reserve(Bt.h_work.size());
+  Bt.mix_off.assign(nt, 0);
+  Bt.mix_n64.assign(nt, 0);
+  Bt.mix_n32.assign(nt, 0);
+  long long nskip = 0;
+  for (size_t k = 0; k < nt; ++k) {
+    const BatchType& T = Bt.types[k];
+    const bool light = coop_class(kPairClassL[T.cb][0], kPairClassL[T.cb][1],
+                                  kPairClassL[T.ck][0], kPairClassL[T.ck][1]) < 0;
+    Bt.mix_off[k] = (long long)w.size();
+    w32.clear();
+    for (long long i = 0; i < T.n; ++i) {
+      const int2 pq = Bt.h_work[(size_t)(T.work_off + i)];
+      const double bnd = Bt.h_qmixed[pq.x] * Bt.h_qmixed[pq.y];
+      if (bnd < skip) {
+        ++nskip;
+        continue;
+      }
+      if (light && bnd < fp32)
+        w32.push_back(pq);
+      else
+        w.push_back(pq);
+    }
+    Bt.mix_n64[k] = (long long)w.size() - Bt.mix_off[k];
+    Bt.mix_n32[k] = (long long)w32.size();
+    w.insert(w.end(), w32.begin(), w32.end());
+  }
+  if (!Bt.d_work_mixed &&
+      (s = Bt.alloc((void**)&Bt.d_work_mixed, std::max<size_t>(Bt.h_work.size(), 1) * sizeof(int2),
+                    "cudaMalloc(batch mixed work list)")))
+    return s;
+  GBX_CUDA(cudaMemcpy(Bt.d_work_mixed, w.data(), w.size() * sizeof(int2), cudaMemcpyHostToDevice),
+           "upload batch mixed work list");
+  long long n32 = 0;
+  for (long long v : Bt.mix_n32) n32 += v;
+  Bt.mix_count[0] = (long long)w.size() - n32;
+  Bt.mix_count[1] = n32;
+  Bt.mix_count[2] = nskip;
+  Bt.mix_skip = skip;
+  Bt.mix_fp32 = fp32;
+  batch_drop_mixed_graph(Bt);
+  return GBX_OK;
+}
+
+// The launches of one batch run on stream `st` (class kernels on the auxiliary streams).
+// mixed: the lists of batch_mixed_lists, FP32 lists on the register kernel's FP32 path, and
+// the compact store cleared first when quartets were left out (their values are zero).
+static int enqueue_batch(Batch& Bt, cudaStream_t st, bool mixed = false) {
+  const int nsm = num_sms_of(Bt.device);
+  if (mixed && Bt.mix_count[2] > 0)
+    GBX_CUDA(cudaMemsetAsync(Bt.d_compact, 0, (size_t)Bt.compact_elems * sizeof(double), st),
+             "clear batch compact store");
   GBX_CUDA(cudaEventRecord(Bt.fork, st), "fork");
   for (cudaStream_t a : Bt.aux) GBX_CUDA(cudaStreamWaitEvent(a, Bt.fork, 0), "fork wait");
   for (size_t i = 0; i < Bt.order.size(); ++i) {
-    const BatchType& T = Bt.types[Bt.order[i]];
+    const int k = Bt.order[i];
+    const BatchType& T = Bt.types[k];
     if (Bt.profile) GBX_CUDA(cudaEventRecord(Bt.type_ev[i], st), "type event");
     EriLaunch a;
     memset(&a, 0, sizeof(a));
@@ -315,12 +480,29 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st) {
     a.team = T.team;
     a.mol_base = T.d_base;
     a.mol_ncols = T.d_ncols;
-    const int grid = (int)std::max<long long>(
-        1, std::min<long long>((T.n * T.team + 127) / 128, (long long)nsm * 8));
-    int s = launch_class(kPairClassL[T.cb][0], kPairClassL[T.cb][1], kPairClassL[T.ck][0],
-                         kPairClassL[T.ck][1], a, grid,
-                         Bt.profile ? st : Bt.aux[i % Bt.aux.size()]);
-    if (s) return s;
+    cudaStream_t ts = Bt.profile ? st : Bt.aux[i % Bt.aux.size()];
+    if (mixed) {
+      a.work = Bt.d_work_mixed;
+      a.work_off = Bt.mix_off[k];
+      a.nwork = Bt.mix_n64[k];
+    }
+    if (a.nwork > 0) {
+      const int grid = (int)std::max<long long>(
+          1, std::min<long long>((a.nwork * T.team + 127) / 128, (long long)nsm * 8));
+      int s = launch_class(kPairClassL[T.cb][0], kPairClassL[T.cb][1], kPairClassL[T.ck][0],
+                           kPairClassL[T.ck][1], a, grid, ts);
+      if (s) return s;
+    }
+    if (mixed && Bt.mix_n32[k] > 0) {  // the type's FP32 list
+      a.work_off = Bt.mix_off[k] + Bt.mix_n64[k];
+      a.nwork = Bt.mix_n32[k];
+      a.fp32 = 1;
+      const int grid = (int)std::max<long long>(
+          1, std::min<long long>((a.nwork * T.team + 127) / 128, (long long)nsm * 8));
+      int s = launch_class(kPairClassL[T.cb][0], kPairClassL[T.cb][1], kPairClassL[T.ck][0],
+                           kPairClassL[T.ck][1], a, grid, ts);
+      if (s) return s;
+    }
   }
   if (Bt.profile) GBX_CUDA(cudaEventRecord(Bt.type_ev[Bt.order.size()], st), "type event");
   for (size_t j = 0; j < Bt.aux.size(); ++j) {
@@ -331,7 +513,9 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st) {
                              Bt.max_row_bytes, st);
 }
 
-static int run_batch(Batch& Bt, int notation, double* const* outs, cudaStream_t caller) {
+// mixed: thresholds (skip, fp32) of the mixed form, nullptr for the FP64 form.
+static int run_batch(Batch& Bt, int notation, double* const* outs, cudaStream_t caller,
+                     const double* mixed = nullptr) {
   for (int m = 0; m < Bt.nmol; ++m)
     if (!outs[m]) return set_error(GBX_ERR_INVALID, "output of molecule %d is null", m);
   bool changed = Bt.exp_dirty;
@@ -349,10 +533,17 @@ static int run_batch(Batch& Bt, int notation, double* const* outs, cudaStream_t 
     GBX_CUDA(cudaStreamSynchronize(Bt.exec), "upload batch descriptors");
     Bt.exp_dirty = false;
   }
+  const bool mx = mixed != nullptr;
+  if (mx) {
+    const int s = batch_mixed_lists(Bt, mixed[0], mixed[1]);
+    if (s) return s;
+  }
+  cudaGraph_t& graph_ref = mx ? Bt.graph_m : Bt.graph;
+  cudaGraphExec_t& exec_ref = mx ? Bt.graph_exec_m : Bt.graph_exec;
   const bool graph = Bt.use_graph && !Bt.profile;
-  if (graph && !Bt.graph_exec) {
+  if (graph && !exec_ref) {
     GBX_CUDA(cudaStreamBeginCapture(Bt.exec, cudaStreamCaptureModeRelaxed), "begin capture");
-    const int s = enqueue_batch(Bt, Bt.exec);
+    const int s = enqueue_batch(Bt, Bt.exec, mx);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(Bt.exec, &g);
     if (s) {
@@ -360,13 +551,13 @@ static int run_batch(Batch& Bt, int notation, double* const* outs, cudaStream_t 
       return s;
     }
     GBX_CUDA(e, "end capture");
-    Bt.graph = g;
-    GBX_CUDA(cudaGraphInstantiate(&Bt.graph_exec, g, 0), "instantiate batch graph");
+    graph_ref = g;
+    GBX_CUDA(cudaGraphInstantiate(&exec_ref, g, 0), "instantiate batch graph");
   }
   if (graph) {
-    GBX_CUDA(cudaGraphLaunch(Bt.graph_exec, Bt.exec), "launch batch graph");
+    GBX_CUDA(cudaGraphLaunch(exec_ref, Bt.exec), "launch batch graph");
   } else {
-    const int s = enqueue_batch(Bt, Bt.exec);
+    const int s = enqueue_batch(Bt, Bt.exec, mx);
     if (s) return s;
   }
   GBX_CUDA(cudaEventRecord(Bt.ev_out, Bt.exec), "record batch");
@@ -431,6 +622,7 @@ static void batch_drop_graph(Batch& B) {
   if (B.graph) cudaGraphDestroy(B.graph);
   B.graph_exec = nullptr;
   B.graph = nullptr;
+  batch_drop_mixed_graph(B);
 }
 
 int gbx_batch_num_types(const gbx_batch* b, int* n) {
@@ -504,4 +696,27 @@ int gbx_batch_run(gbx_batch* b, int notation, double* const* outs, void* stream)
   Batch& B = *b->impl;
   DeviceGuardLite g(B.device);
   return run_batch(B, notation, outs, (cudaStream_t)stream);
+}
+
+int gbx_batch_run_mixed(gbx_batch* b, int notation, double skip, double fp32,
+                        double* const* outs, void* stream) {
+  if (!b || !outs) return set_error(GBX_ERR_INVALID, "gbx_batch_run_mixed: null argument");
+  if (notation != GBX_CHEMIST && notation != GBX_PHYSICIST)
+    return set_error(GBX_ERR_INVALID, "notation must be GBX_CHEMIST or GBX_PHYSICIST");
+  if (!(skip >= 0.0) || !(fp32 >= 0.0))
+    return set_error(GBX_ERR_INVALID, "thresholds must be >= 0");
+  Batch& B = *b->impl;
+  DeviceGuardLite g(B.device);
+  const double th[2] = {skip, fp32};
+  return run_batch(B, notation, outs, (cudaStream_t)stream, th);
+}
+
+int gbx_batch_mixed_counts(const gbx_batch* b, int64_t* n_fp64, int64_t* n_fp32,
+                           int64_t* n_skipped) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_batch_mixed_counts: null batch");
+  const Batch& B = *b->impl;
+  if (n_fp64) *n_fp64 = B.mix_count[0];
+  if (n_fp32) *n_fp32 = B.mix_count[1];
+  if (n_skipped) *n_skipped = B.mix_count[2];
+  return GBX_OK;
 }

@@ -714,6 +714,15 @@ __global__ void diagonal_bounds(const PairDev* __restrict__ pairs, int npairs,
   q[p] = sqrt(mx);
 }
 
+// diagonal_bounds for one molecule of a batch (its pairs, block table and compact store).
+int launch_diagonal_bounds(const PairDev* pairs, int npairs, const ShellDev* shells,
+                           const BlockDev* blocks, const double* compact, double* q,
+                           cudaStream_t st) {
+  if (npairs <= 0) return GBX_OK;
+  diagonal_bounds<<<(npairs + 127) / 128, 128, 0, st>>>(pairs, npairs, shells, blocks, compact, q);
+  return cuda_status(cudaGetLastError(), "diagonal_bounds launch");
+}
+
 // Bounds of the final values for the mixed form: every output integral satisfies
 // |(ab|cd)| <= sqrt((ab|ab) (cd|cd)) <= Q_p Q_q (Cauchy-Schwarz for the output functions
 // themselves: norm_cont, component norms and spherical transforms included).  The diagonal

@@ -132,6 +132,9 @@ int launch_expand_batch(int device, const ExpandArgs* d_mols, const long long* d
                         int nmol, long long total_rows, size_t max_row_bytes, cudaStream_t st);
 ExpandArgs make_expand_args(const Basis& B, int notation, double* out);
 int num_sms_of(int device);
+int launch_diagonal_bounds(const PairDev* pairs, int npairs, const ShellDev* shells,
+                           const BlockDev* blocks, const double* compact, double* q,
+                           cudaStream_t st);
 int launch_class(int la, int lb, int lc, int ld, const EriLaunch& a, int grid, cudaStream_t st);
 
 }  // namespace gbx

@@ -184,6 +184,17 @@ int gbx_batch_type_info(const gbx_batch* b, int k, int* cls4, int* team, double*
 int gbx_batch_set_team(gbx_batch* b, int k, int team);
 int gbx_batch_set_profiling(gbx_batch* b, int on);
 int gbx_batch_type_times(gbx_batch* b, double* ms, int n);
+/* Mixed-precision form of gbx_batch_run (the batched counterpart of gbx_eri_full_mixed; no
+ * counterpart in the reference, which has neither batches nor a mixed form): quartets whose
+ * final-value bound Q_p Q_q is below `skip` are zero, those below `fp32` in light classes run
+ * their recursions in FP32.  The bounds are computed once per batch (first mixed run; make it
+ * before any stream capture), the lists once per pair of thresholds; the mixed launches are
+ * captured into their own CUDA graph.  gbx_batch_mixed_counts: quartets of the last lists in
+ * FP64, in FP32 and left out (all 0 before the first mixed run). */
+int gbx_batch_run_mixed(gbx_batch* b, int notation, double skip, double fp32,
+                        double* const* outs, void* stream);
+int gbx_batch_mixed_counts(const gbx_batch* b, int64_t* n_fp64, int64_t* n_fp32,
+                           int64_t* n_skipped);
 
 /* Coulomb matrix J[a,b] = sum_cd (ab|cd) D[c,d] from the screened unique quartets
  * (full tensor never stored).  D, J: device N x N row-major (D symmetric). */

@@ -108,3 +108,53 @@ def test_batch_autotuner_keeps_values():
     for o, r in zip(outs, ref):
         np.testing.assert_allclose(o.cpu().numpy(), r.cpu().numpy(), rtol=0, atol=1e-13)
     b.close()
+
+
+def _stretched(mol, f):
+    from gbasis_b200.contractions import GeneralizedContractionShell
+    return [GeneralizedContractionShell(s.angmom, np.asarray(s.coord) * f, np.asarray(s.coeffs),
+                                        np.asarray(s.exps), s.coord_type) for s in mol]
+
+
+def test_batch_mixed_form_against_fp64_and_single_path():
+    """Mixed form of the batch: within 1e-10 of the FP64 batch, equal (1e-12) to the
+    single-basis mixed form of each molecule, graph replay reproducible, and the FP64 graph
+    unaffected.  Two molecules are stretched (x4, x3) so that the batch has quartets left out
+    (bounds far below 1e-11) and FP32 quartets (light-class bounds in [1e-9, 2e-8])."""
+    import ctypes
+    import torch
+    from gbasis_b200.electron_repulsion import MIXED_FP32, MIXED_SKIP
+    mols = [batch_molecule(m) for m in range(60, 66)]
+    mols += [_stretched(batch_molecule(68), 4.0), _stretched(batch_molecule(71), 3.0)]
+    b = EriBatch(mols)
+    th = (MIXED_SKIP, MIXED_FP32)
+
+    def fresh():
+        return [torch.full((n,) * 4, np.nan, dtype=torch.float64, device="cuda") for n in b.nbf]
+    o64, omx, omx2, o64b = fresh(), fresh(), fresh(), fresh()
+    b.run(o64)
+    b.run(omx, mixed=th)
+    b.run(omx2, mixed=th)  # replay of the mixed graph
+    b.run(o64b)  # FP64 graph after the mixed runs
+    torch.cuda.synchronize()
+    n64, n32, nskip = b.mixed_counts()
+    assert n64 + n32 + nskip == b.n_quartets
+    assert n32 > 0 and nskip > 0
+    for m, shells in enumerate(mols):
+        ref = o64[m].cpu().numpy()
+        got = omx[m].cpu().numpy()
+        assert np.isfinite(got).all()
+        assert np.max(np.abs(got - ref)) <= 1e-10, m
+        np.testing.assert_array_equal(omx2[m].cpu().numpy(), got)
+        np.testing.assert_array_equal(o64b[m].cpu().numpy(), ref)
+        db = _engine.DeviceBasis(shells)
+        single = torch.empty(db.nbf ** 4, dtype=torch.float64, device="cuda")
+        db.full_device(single.data_ptr(), "chemist", 0.0,
+                       stream=ctypes.c_void_p(torch.cuda.current_stream().cuda_stream), mixed=th)
+        torch.cuda.synchronize()
+        db.close()
+        np.testing.assert_allclose(got.reshape(-1), single.cpu().numpy(), rtol=0, atol=1e-12)
+    b.close()
+    outs = electron_repulsion_integral_batch(mols[:2], notation="chemist", precision="mixed")
+    for o, ref in zip(outs, o64[:2]):
+        assert float((o - ref).abs().max()) <= 1e-10
