@@ -225,7 +225,7 @@ def extra_configs(local, reps=2):
       atom), N = 420; the 8-fold unique integrals only (no N^4 tensor), FP64 and mixed form,
       with the mixed form's max error over the whole compact store;
     * ``batch512``: 512 molecules of 2-14 atoms, one CUDA graph per run (every molecule's full
-      Cartesian tensor, device resident);
+      Cartesian tensor, device resident), FP64 and mixed form side by side;
     * ``large64_coulomb_subset``: direct Coulomb matrix of the first 16 atoms of the 64-atom
       box (160 spherical shells, N = 480; the full 64-atom system takes minutes).
     """
@@ -292,6 +292,28 @@ def extra_configs(local, reps=2):
         "value": uq / (ms * 1e-3), "unit": UNIT, "molecules_per_s": len(mols) / (ms * 1e-3),
         "achieved_tflops": fl / (ms * 1e-3) / 1e12, "frac_fp64_peak": fl / (ms * 1e-3) / 1e12 / peak64,
         "create_s": t_create, "launch": "one CUDA graph replay per run"}
+    # mixed form of the same batch, side by side (its own graph); error against the FP64
+    # tensors of every 8th molecule with N <= 80
+    try:
+        th = (MIXED_SKIP, MIXED_FP32)
+        sample = [m for m in range(0, len(mols), 8) if b.nbf[m] <= 80]
+        ref = {m: outs[m].clone() for m in sample}
+        t0 = time.perf_counter()
+        b.run(outs, stream=sp, mixed=th)  # first mixed run: bounds and lists
+        torch.cuda.synchronize()
+        t_setup = time.perf_counter() - t0
+        ms_mx = timed(lambda: b.run(outs, stream=sp, mixed=th))
+        err = max(float((outs[m] - ref[m]).abs().max()) for m in sample)
+        n64, n32, nskip = b.mixed_counts()
+        out["batch512"]["mixed"] = {
+            "ms": ms_mx, "value": uq / (ms_mx * 1e-3), "unit": UNIT,
+            "speedup_vs_fp64": ms / ms_mx, "max_abs_err_vs_fp64": err,
+            "error_over": f"full tensors of {len(sample)} molecules (every 8th with N <= 80)",
+            "quartets_fp64": n64, "quartets_fp32": n32, "quartets_left_out": nskip,
+            "first_run_s": t_setup, "skip_bound": MIXED_SKIP, "fp32_bound": MIXED_FP32}
+        del ref
+    except Exception as exc:  # keep the rest of the line
+        out["batch512"]["mixed"] = {"error": str(exc)[:300]}
     b.close()
     del outs
     torch.cuda.empty_cache()

@@ -212,11 +212,13 @@ def potential_code(potential="coulomb", omega=None):
 
 # Mixed form thresholds on B_pq = Q_p Q_q, Q_p = sqrt(max |(ab|ab)|) over the pair's output
 # functions (a rigorous bound on |(ab|cd)|).  Skipped quartets contribute at most MIXED_SKIP;
-# the FP32 recursions lose up to ~1e-4 of B_pq on f-containing classes (measured: 20-atom
-# s/p/d/f chain, max error 1.2e-11 at 2e-7, 1.3e-10 at 1e-6), so the FP32 bound keeps the sum
-# below 1e-10 with margin.
+# an FP32 quartet's error is a fraction of its B_pq that depends on the molecule: about 1e-4
+# on the 20-atom s/p/d/f chain (max error 1.2e-11 at an FP32 bound of 2e-7, 1.3e-10 at 1e-6),
+# 1.6e-3 on the synthetic 2-14-atom s/p/d molecules with up to 6 primitives (3.2e-10 at 2e-7).
+# The FP32 bound of 1e-8 keeps both below 1e-10 with margin; lowering it only moves quartets
+# to FP64, so the error can only shrink.
 MIXED_SKIP = 1e-11
-MIXED_FP32 = 2e-7
+MIXED_FP32 = 1e-8
 
 
 def electron_repulsion_integral(basis, transform=None, notation="physicist", *, coord_type=None,
