@@ -136,6 +136,18 @@ def replica_throughput(world, units_per_rank, ms):
     return world * units_per_rank / (ms * 1e-3)
 
 
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.machine()
+
+
 def cpu_baseline(shells, seconds=12.0, seed=0):
     """Oracle on a seeded random sample of unique shell quartets, extrapolated."""
     import itertools
@@ -156,6 +168,7 @@ def cpu_baseline(shells, seconds=12.0, seed=0):
     from gbasis_b200.flops import unique_eris
     est_total = dt / done * nq
     return {"value": unique_eris(n) / est_total, "unit": UNIT, "cores": 1, "kind": "port",
+            "host_cpus": os.cpu_count(), "cpu_model": _cpu_model(),
             "sample": f"{done} random unique shell quartets of {nq} ({dt:.1f} s, "
                       f"oracle construct_array_contraction, 1 core), extrapolated"}
 
@@ -211,6 +224,7 @@ def run_reference(a, rank, world):
             "config": {"workload": WORKLOAD, "n_functions": n, "shell_quartets": nq,
                        "notation": "physicist", "coord_type": "cartesian"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "cpu_model": _cpu_model(),
                              "sample": f"{per_step:.0f} s per step per core of random unique "
                                        f"shell quartets, extrapolated to {nq} quartets"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -499,7 +513,10 @@ def main():
     if world == 1 and not a.no_extra_configs:
         del out
         torch.cuda.empty_cache()
-        line["configs"] = extra_configs(local)
+        try:  # the secondary configurations never cost the headline line
+            line["configs"] = extra_configs(local)
+        except Exception as exc:
+            line["configs"] = {"error": str(exc)[:300]}
     if rank == 0 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(shells)
     if rank == 0:
