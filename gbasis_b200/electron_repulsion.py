@@ -154,6 +154,29 @@ class ElectronRepulsionIntegralImproved(ElectronRepulsionIntegral):
         super().__init__(contractions)
         self._screen = float(schwarz_threshold)
 
+    @classmethod
+    def construct_array_contraction(cls, cont_one, cont_two, cont_three, cont_four, **kwargs):
+        """As :meth:`ElectronRepulsionIntegral.construct_array_contraction`, with the screening
+        hook of ``electron_repulsion.py:306-360``: given ``screener`` (an object with
+        ``is_significant(i, j, k, l)``, such as :class:`~gbasis_b200.schwarz_screening.
+        SchwarzScreener`) and ``contraction_index_map`` (``{id(shell): shell index}``), a
+        quartet the screener rejects is returned as zeros without a device call."""
+        shells = (cont_one, cont_two, cont_three, cont_four)
+        for name, c in zip(("cont_one", "cont_two", "cont_three", "cont_four"), shells):
+            if not is_shell(c):
+                raise TypeError(f"`{name}` must be a `GeneralizedContractionShell` instance.")
+        screener = kwargs.get("screener")
+        index_map = kwargs.get("contraction_index_map")
+        if screener is not None and index_map is not None:
+            idx = [index_map.get(id(c)) for c in shells]
+            if None not in idx and not screener.is_significant(*idx):
+                shape = []
+                for c in shells:
+                    cf = np.asarray(c.coeffs)
+                    shape += [cf.shape[1] if cf.ndim == 2 else 1, len(c.angmom_components_cart)]
+                return np.zeros(shape)
+        return super().construct_array_contraction(*shells)
+
 
 def _lincomb_device(shells, types, transform, screen, device, potential=(0, 0.0)):
     import ctypes

@@ -39,3 +39,25 @@ def test_screener_counts_match_reference():
         assert st["total"] == len(pairs) * (len(pairs) + 1) // 2
         scr.reset_counters()
         assert scr.get_statistics()["total"] == 0
+
+
+def test_improved_contraction_with_screener():
+    """The screening hook of ``ElectronRepulsionIntegralImproved.construct_array_contraction``
+    with the device screener: rejected quartets are zeros, the others equal the plain call."""
+    from gbasis_b200.electron_repulsion import ElectronRepulsionIntegral
+    from gbasis_b200.electron_repulsion import ElectronRepulsionIntegralImproved as Imp
+    z = load_npz("schwarz.npz")
+    shells = shells_from_json(z["shells"])
+    scr = sz.SchwarzScreener(shells, None, None, 1e-3)
+    index_map = {id(s): i for i, s in enumerate(shells)}
+    q = scr.bounds
+    for (i, j, k, l) in [(0, 1, 2, 3), (0, 4, 0, 5), (2, 2, 1, 0)]:
+        sh = (shells[i], shells[j], shells[k], shells[l])
+        blk = Imp.construct_array_contraction(*sh, screener=scr, contraction_index_map=index_map)
+        if q[i, j] * q[k, l] < 1e-3:
+            assert not blk.any()
+        else:
+            ref = ElectronRepulsionIntegral.construct_array_contraction(*sh)
+            np.testing.assert_allclose(blk, ref, rtol=0, atol=1e-14)
+    assert scr.get_statistics() == {"n_screened": 1, "n_computed": 2, "total": 3,
+                                    "percent_screened": 100.0 / 3, "speedup_factor": 1.5}

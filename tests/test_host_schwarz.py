@@ -50,3 +50,28 @@ def test_argument_checks():
         sz.compute_schwarz_bounds([])
     with pytest.raises(TypeError):
         sz.SchwarzScreener([object()])
+
+
+def test_improved_contraction_screening_hook_without_device():
+    # gbasis/integrals/electron_repulsion.py:340-360: a rejected quartet is zeros of the
+    # block's shape, (M1, L1, M2, L2, M3, L3, M4, L4); nothing reaches the device
+    from gbasis_b200.electron_repulsion import ElectronRepulsionIntegralImproved as Imp
+    z, shells = _fixture()
+
+    class Reject:
+        calls = []
+
+        def is_significant(self, i, j, k, l_shell):
+            self.calls.append((i, j, k, l_shell))
+            return False
+    scr = Reject()
+    index_map = {id(s): i for i, s in enumerate(shells)}
+    blk = Imp.construct_array_contraction(shells[2], shells[3], shells[1], shells[0],
+                                          screener=scr, contraction_index_map=index_map)
+    m = [np.asarray(s.coeffs).shape[1] for s in shells]
+    assert blk.shape == (m[2], 6, m[3], 10, m[1], 3, m[0], 1)
+    assert not blk.any()
+    assert scr.calls == [(2, 3, 1, 0)]
+    with pytest.raises(TypeError):
+        Imp.construct_array_contraction(None, shells[0], shells[0], shells[0], screener=scr,
+                                        contraction_index_map=index_map)
