@@ -148,8 +148,9 @@ def _cpu_model():
     return platform.machine()
 
 
-def cpu_baseline(shells, seconds=12.0, seed=0):
-    """Oracle on a seeded random sample of unique shell quartets, extrapolated."""
+def cpu_baseline(shells, seconds=12.0, seed=0, n_functions=None):
+    """Oracle on a seeded random sample of unique shell quartets, extrapolated (unique ERIs
+    counted over ``n_functions``, default the Cartesian functions)."""
     import itertools
     from oracle import eri_oracle as orc
     pairs = list(itertools.combinations_with_replacement(range(len(shells)), 2))
@@ -164,7 +165,7 @@ def cpu_baseline(shells, seconds=12.0, seed=0):
         orc.construct_array_contraction(shells[i], shells[j], shells[k], shells[l])
         done += 1
     dt = time.perf_counter() - t0
-    n = sum(len(s.angmom_components_cart) for s in shells)
+    n = n_functions or sum(len(s.angmom_components_cart) for s in shells)
     from gbasis_b200.flops import unique_eris
     est_total = dt / done * nq
     return {"value": unique_eris(n) / est_total, "unit": UNIT, "cores": 1, "kind": "port",
@@ -289,6 +290,11 @@ def extra_configs(local, reps=2):
                   "error_over": "every unique integral", "skip_bound": MIXED_SKIP,
                   "fp32_bound": MIXED_FP32}}
     del ref, cur, r, x, d
+    try:  # the oracle's Cartesian blocks on a sample of this workload's quartets, 1 core
+        out["chain20_unique"]["cpu_baseline"] = cpu_baseline(shells, seconds=8.0, seed=3,
+                                                             n_functions=db.nbf)
+    except Exception as exc:
+        out["chain20_unique"]["cpu_baseline"] = {"error": str(exc)[:300]}
     db.close()
     torch.cuda.empty_cache()
 
