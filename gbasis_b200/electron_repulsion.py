@@ -177,6 +177,65 @@ class ElectronRepulsionIntegralImproved(ElectronRepulsionIntegral):
                 return np.zeros(shape)
         return super().construct_array_contraction(*shells)
 
+    def _screen_from(self, kwargs):
+        """Threshold of a whole-array call given the reference's screener hook.
+
+        gbasis's whole-array methods pass ``screener`` and ``contraction_index_map`` to every
+        ``construct_array_contraction`` call of their loop over unique shell quartets
+        ((i, j) <= (k, l) over pairs i <= j, ``base_four_symm.py:189-191``).  Here the device
+        zeroes the quartets with Q_ij Q_kl below ``screener.threshold`` in one pass, and the
+        screener's counters grow as that loop would make them grow."""
+        screener = kwargs.pop("screener", None)
+        index_map = kwargs.pop("contraction_index_map", None)
+        if kwargs:
+            raise TypeError(f"unexpected keyword arguments: {', '.join(sorted(kwargs))}")
+        if screener is None or index_map is None:
+            return self._screen
+        n = len(self.contractions)
+        if [index_map.get(id(c)) for c in self.contractions] != list(range(n)):
+            raise NotImplementedError("`contraction_index_map` must number the instance's "
+                                      "shells 0..n-1 in order")
+        t = float(screener.threshold)
+        qp = np.sort(np.asarray(screener.bounds, dtype=float)[np.triu_indices(n)])
+        npair = len(qp)
+        total = npair * (npair + 1) // 2
+        if t <= 0.0:
+            computed = total
+        else:
+            # ordered pairs (a, b) with q_a q_b >= t, then unordered with a == b allowed
+            pos = qp[qp > 0.0]
+            need = t / pos
+            ordered = int(np.sum(len(qp) - np.searchsorted(qp, need, side="left")))
+            diag = int(np.count_nonzero(qp * qp >= t))
+            computed = (ordered + diag) // 2
+        screener.n_computed += computed
+        screener.n_screened += total - computed
+        return max(self._screen, t)
+
+    def _screened(self, kwargs, call):
+        saved = self._screen
+        self._screen = self._screen_from(dict(kwargs))
+        try:
+            return call()
+        finally:
+            self._screen = saved
+
+    def construct_array_cartesian(self, out=None, device=None, **kwargs):
+        return self._screened(kwargs, lambda: super(ElectronRepulsionIntegralImproved, self)
+                              .construct_array_cartesian(out, device))
+
+    def construct_array_spherical(self, out=None, device=None, **kwargs):
+        return self._screened(kwargs, lambda: super(ElectronRepulsionIntegralImproved, self)
+                              .construct_array_spherical(out, device))
+
+    def construct_array_mix(self, coord_types, out=None, device=None, **kwargs):
+        return self._screened(kwargs, lambda: super(ElectronRepulsionIntegralImproved, self)
+                              .construct_array_mix(coord_types, out, device))
+
+    def construct_array_lincomb(self, transform, coord_type, device=None, **kwargs):
+        return self._screened(kwargs, lambda: super(ElectronRepulsionIntegralImproved, self)
+                              .construct_array_lincomb(transform, coord_type, device))
+
 
 def _lincomb_device(shells, types, transform, screen, device, potential=(0, 0.0)):
     import ctypes

@@ -61,3 +61,21 @@ def test_improved_contraction_with_screener():
             np.testing.assert_allclose(blk, ref, rtol=0, atol=1e-14)
     assert scr.get_statistics() == {"n_screened": 1, "n_computed": 2, "total": 3,
                                     "percent_screened": 100.0 / 3, "speedup_factor": 1.5}
+
+
+def test_whole_array_screener_hook():
+    """``construct_array_cartesian(screener=..., contraction_index_map=...)`` of the improved
+    class: the same array as a Schwarz threshold equal to the screener's, and the screener's
+    counts equal to those of the reference's own screener on this basis."""
+    from gbasis_b200.electron_repulsion import ElectronRepulsionIntegralImproved as Imp
+    z = load_npz("schwarz.npz")
+    shells = shells_from_json(z["shells"])
+    scr = sz.SchwarzScreener(shells, None, None, 1e-3)
+    obj = Imp(shells)
+    got = obj.construct_array_cartesian(screener=scr,
+                                        contraction_index_map={id(s): i
+                                                               for i, s in enumerate(shells)})
+    assert obj._screen == 0.0
+    ref = Imp(shells, 1e-3).construct_array_cartesian()
+    np.testing.assert_array_equal(got, ref)
+    np.testing.assert_array_equal([scr.n_screened, scr.n_computed], z["stats_0.001"])

@@ -75,3 +75,45 @@ def test_improved_contraction_screening_hook_without_device():
     with pytest.raises(TypeError):
         Imp.construct_array_contraction(None, shells[0], shells[0], shells[0], screener=scr,
                                         contraction_index_map=index_map)
+
+
+def test_whole_array_screener_counts_match_reference():
+    # the whole-array methods with the reference's hook count as the reference's loop over
+    # unique shell quartets (base_four_symm.py:189-191) counts: the reference's own screener
+    # statistics on the fixture's bounds, and a brute-force loop on random bounds
+    from gbasis_b200.electron_repulsion import ElectronRepulsionIntegralImproved as Imp
+    z, shells = _fixture()
+    index_map = {id(s): i for i, s in enumerate(shells)}
+
+    class Stub:
+        def __init__(self, bounds, t):
+            self.bounds, self.threshold = bounds, t
+            self.n_screened = self.n_computed = 0
+    obj = Imp(shells)
+    for t in z["thresholds"]:
+        st = Stub(z["bounds"], t)
+        assert obj._screen_from({"screener": st, "contraction_index_map": index_map}) == t
+        np.testing.assert_array_equal([st.n_screened, st.n_computed], z[f"stats_{t:g}"])
+    rng = np.random.default_rng(7)
+    n = 9
+    q = rng.lognormal(-3.0, 3.0, size=(n, n))
+    q = np.triu(q) + np.triu(q, 1).T
+    pairs = [(i, j) for i in range(n) for j in range(i, n)]
+    s0 = shells[0]
+    many = [type(s0)(s0.angmom, s0.coord + i, s0.coeffs, s0.exps, s0.coord_type)
+            for i in range(n)]
+    objn = Imp(many)
+    many_map = {id(s): i for i, s in enumerate(many)}
+    for t in (1e-10, 1e-6, 1e-3, 0.0):
+        brute = sum(q[i, j] * q[k, l] >= t for p, (i, j) in enumerate(pairs)
+                    for (k, l) in pairs[p:])
+        st = Stub(q, t)
+        objn._screen_from({"screener": st, "contraction_index_map": many_map})
+        assert st.n_computed == brute
+        assert st.n_screened == len(pairs) * (len(pairs) + 1) // 2 - brute
+    with pytest.raises(NotImplementedError):
+        obj._screen_from({"screener": Stub(z["bounds"], 1e-3),
+                          "contraction_index_map": {id(s): len(shells) - 1 - i
+                                                    for i, s in enumerate(shells)}})
+    with pytest.raises(TypeError):
+        obj._screen_from({"bad_keyword": 3})
