@@ -39,3 +39,26 @@ def test_point_charge_argument_checks():
         pc.nuclear_electron_attraction_integral(basis, np.zeros((2, 3)), np.ones(3))
     with pytest.raises(TypeError):
         pc.point_charge_integral([object()], np.zeros((1, 3)), np.ones(1))
+
+
+def test_reference_module_paths():
+    # gbasis.integrals.<module> -> gbasis_b200.integrals.<module>, same names, same objects
+    import importlib
+    from gbasis_b200 import electron_repulsion, point_charge, schwarz_screening
+    expect = {
+        "electron_repulsion": (electron_repulsion, ["ElectronRepulsionIntegral",
+                                                    "ElectronRepulsionIntegralImproved",
+                                                    "electron_repulsion_integral",
+                                                    "electron_repulsion_integral_improved"]),
+        "_schwarz_screening": (schwarz_screening, ["compute_schwarz_bound_shell_pair",
+                                                   "compute_schwarz_bounds",
+                                                   "shell_pair_significant", "SchwarzScreener"]),
+        "point_charge": (point_charge, ["point_charge_integral"]),
+        "nuclear_electron_attraction": (point_charge, ["nuclear_electron_attraction_integral"]),
+    }
+    for mod, (src, names) in expect.items():
+        m = importlib.import_module(f"gbasis_b200.integrals.{mod}")
+        for name in names:
+            assert getattr(m, name) is getattr(src, name)
+    from gbasis_b200.contractions import GeneralizedContractionShell  # gbasis.contractions
+    assert GeneralizedContractionShell.__name__ == "GeneralizedContractionShell"
