@@ -62,3 +62,38 @@ def test_reference_module_paths():
             assert getattr(m, name) is getattr(src, name)
     from gbasis_b200.contractions import GeneralizedContractionShell  # gbasis.contractions
     assert GeneralizedContractionShell.__name__ == "GeneralizedContractionShell"
+
+
+def test_no_cpu_fallback_without_library_or_device():
+    """The engine has no CPU path: without its library the call raises ImportError, and where
+    the library loads but no CUDA device answers (as on a CPU-only machine) it raises
+    EngineError instead of returning anything."""
+    import subprocess
+    import sys
+    code = r'''
+import sys
+sys.path.insert(0, sys.argv[1])
+from gbasis_b200 import _engine
+from gbasis_b200 import electron_repulsion as er
+from gbasis_b200.synthetic import make_workload
+shells = make_workload("tiny4")
+_engine.LIB_PATH = "/nonexistent/libgbx_eri.so"
+_engine._lib = None
+try:
+    er.electron_repulsion_integral(shells)
+    print("RETURNED")
+except ImportError:
+    print("IMPORTERROR")
+'''
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code, root], capture_output=True, text=True,
+                         timeout=300)
+    assert out.stdout.strip().splitlines()[-1] == "IMPORTERROR", out.stdout + out.stderr
+    from gbasis_b200 import _engine
+    import torch
+    if os.path.exists(_engine.LIB_PATH) and not torch.cuda.is_available():
+        from gbasis_b200 import electron_repulsion as er
+        from gbasis_b200.synthetic import make_workload
+        with pytest.raises(_engine.EngineError):
+            er.electron_repulsion_integral(make_workload("tiny4"))
