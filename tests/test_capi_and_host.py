@@ -84,7 +84,17 @@ def _pyexec(lines, env):
     exec("\n".join(code), env)
 
 
-@pytest.mark.parametrize("cls", gen_eri.canonical_classes(2))
+# The straight-line register code that the device compiles: every light class and the (ab|ss)
+# structs of the point-charge kernel (the heavy classes run the line, split and cooperative
+# kernels, whose generated code is checked in tests/test_lines_host.py and below); plus every
+# class with l <= 2.
+_REGISTER_CLASSES = sorted(
+    set(gen_eri.canonical_classes(2))
+    | {c for c in gen_eri.canonical_classes(3) if gen_eri.is_light(c)}
+    | {(la, lb, 0, 0) for la in range(4) for lb in range(4)})
+
+
+@pytest.mark.parametrize("cls", _REGISTER_CLASSES)
 def test_generated_recursions_match_oracle(cls):
     la, lb, lc, ld = cls
     rng = np.random.default_rng(sum((i + 1) * v for i, v in enumerate(cls)))
