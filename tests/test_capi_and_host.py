@@ -94,6 +94,12 @@ _REGISTER_CLASSES = sorted(
     | {(la, lb, 0, 0) for la in range(4) for lb in range(4)})
 
 
+def test_register_emitter_refuses_classes_beyond_its_checked_range():
+    assert max(sum(c) for c in _REGISTER_CLASSES) <= gen_eri.MAX_EMIT_L
+    with pytest.raises(ValueError):
+        gen_eri.emit_all(3, [(3, 3, 3, 3)])
+
+
 @pytest.mark.parametrize("cls", _REGISTER_CLASSES)
 def test_generated_recursions_match_oracle(cls):
     la, lb, lc, ld = cls
