@@ -33,7 +33,7 @@ EXPORTED_SYMBOLS = (
     "gbx_batch_set_graph", "gbx_unique_values", "gbx_compact_view",
     "gbx_batch_num_types", "gbx_batch_type_info", "gbx_batch_set_team", "gbx_batch_set_profiling",
     "gbx_batch_type_times", "gbx_release_cached_memory", "gbx_eri_jk", "gbx_point_charge",
-    "gbx_basis_set_potential", "gbx_batch_run_mixed", "gbx_batch_mixed_counts",
+    "gbx_basis_set_potential", "gbx_batch_run_mixed", "gbx_batch_mixed_counts", "gbx_boys_eval",
 )
 
 
@@ -78,6 +78,7 @@ def lib():
             "gbx_last_counts": [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
             "gbx_last_error": [ctypes.c_char_p, ctypes.c_size_t],
             "gbx_fp64_peak": [_I, ctypes.POINTER(_D)],
+            "gbx_boys_eval": [_I, _I64, _P, _P],
             "gbx_set_profiling": [_P, _I],
             "gbx_phase_times": [_P, _P],
             "gbx_eri_full_noalloc": [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
@@ -405,3 +406,12 @@ def fp64_peak(device=0):
     v = ctypes.c_double()
     check(lib().gbx_fp64_peak(int(device), ctypes.byref(v)), "gbx_fp64_peak")
     return float(v.value)
+
+
+def boys_eval(m_max, T):
+    """F_0..F_{m_max}(T) for each T (n x (m_max + 1)) from the device Boys function the class
+    kernels use (``gbx_boys_eval``)."""
+    T = np.ascontiguousarray(T, dtype=np.float64).reshape(-1)
+    F = np.empty((T.size, int(m_max) + 1), dtype=np.float64)
+    check(lib().gbx_boys_eval(int(m_max), T.size, _ptr(T), _ptr(F)), "gbx_boys_eval")
+    return F

@@ -41,7 +41,7 @@ def sources(lmax):
     gen = gen_eri.emit_sources(GEN, lmax)
     return [os.path.join(GEN, g) for g in gen] + [
         os.path.join(CSRC, f) for f in ("runtime.cu", "pipeline.cu", "extras.cu", "noalloc.cu",
-                                        "coop_kernel.cu", "batch.cu", "one_elec.cu")]
+                                        "coop_kernel.cu", "batch.cu", "one_elec.cu", "boys_eval.cu")]
 
 
 KERNEL_DEPS = ("gbx_common.cuh", "eri_kernels.cuh", "errors.h", "_gen/eri_gen.cuh")
@@ -56,7 +56,7 @@ def _deps_mtime(src):
     base = os.path.basename(src)
     deps = (KERNEL_DEPS if base.startswith("eri_cls") else
             LINES_DEPS if base.startswith("lines_") else
-            KERNEL_DEPS + HOST_DEPS if base == "one_elec.cu" else HOST_DEPS)
+            KERNEL_DEPS + HOST_DEPS if base in ("one_elec.cu", "boys_eval.cu") else HOST_DEPS)
     m = os.path.getmtime(os.path.join(ROOT, "include", "gbx_eri.h"))
     for d in deps:
         p = os.path.join(CSRC, d)

@@ -173,7 +173,9 @@ extern "C" int gbx_eri_full_noalloc(int n_shells, const int* angmom, const int* 
   if ((s = cuda_status(cudaGetLastError(), "build_work launch"))) return s;
   int nsm = 1;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  for (int k = 0; k < nblk; ++k) {
+  for (int i = 0; i < nblk; ++i) {
+    // largest blocks first, each with the default lanes per quartet of a basis handle
+    const int k = B.launch_order.empty() ? i : B.launch_order[i];
     const HostBlock& h = B.blocks[k];
     EriLaunch a;
     memset(&a, 0, sizeof(a));
@@ -189,7 +191,9 @@ extern "C" int gbx_eri_full_noalloc(int n_shells, const int* angmom, const int* 
     a.base = h.dev.base;
     a.ncols = h.dev.ncols;
     a.mode = 0;
-    const int grid = (int)std::min<long long>((h.ncand + 127) / 128, (long long)nsm * 8);
+    a.team = h.team;
+    const int grid = (int)std::max<long long>(
+        1, std::min<long long>((h.ncand * h.team + 127) / 128, (long long)nsm * 8));
     if ((s = launch_class(kPairClassL[h.cb][0], kPairClassL[h.cb][1], kPairClassL[h.ck][0],
                           kPairClassL[h.ck][1], a, grid, st)))
       return s;

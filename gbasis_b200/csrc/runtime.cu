@@ -147,6 +147,15 @@ static void cache_give(int device, void* p, size_t bytes) {
 }
 
 Basis::~Basis() {
+  // A basis that never allocated device memory nor created a stream or event (host
+  // bookkeeping only, as the allocation-free entry point uses it) touches no device state
+  // here: no device switch and no device-wide synchronisation.
+  bool owns = !dev_allocs.empty() || fork || copy_stream || !aux.empty() || !join.empty() ||
+              !blk_ev.empty();
+  for (cudaEvent_t e : ev) owns = owns || e;
+  for (cudaEvent_t e : stage_ready) owns = owns || e;
+  for (cudaEvent_t e : stage_free) owns = owns || e;
+  if (!owns) return;
   DeviceGuard g(device);
   // blocks go back to the cache only once nothing queued on the device can still use them
   // (what cudaFree would have waited for)

@@ -252,6 +252,14 @@ int gbx_last_error(char* buf, size_t len);
 /* Sustained FP64 FMA rate of the device (TFLOP/s) from a dependent-FMA microbenchmark. */
 int gbx_fp64_peak(int device, double* tflops);
 
+/* Boys values F_0..F_{m_max}(T[i]) on the current device, computed by the same device
+ * function the class kernels use (Taylor table for T < 40, asymptotic form above), for
+ * checking that function on its own.  Replaces, for that purpose,
+ * boys_function_standard / boys_function_recursion (gbasis/integrals/boys_functions.py:26-63,
+ * :102-142).  T: host, n finite values >= 0 (anything else is GBX_ERR_INVALID); F: host,
+ * n x (m_max + 1) row-major; 0 <= m_max <= 13.  Synchronous. */
+int gbx_boys_eval(int m_max, int64_t n, const double* T, double* F);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,7 +50,7 @@ def parse(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="path of a gbasis source checkout")
     a = ap.parse_args()
     shells, expected = parse(os.path.join(a.reference, "tests", "test_two_elec_int.py"))
 

@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="path of a gbasis source checkout")
     a = ap.parse_args()
     sys.path.insert(0, a.reference)
     from gbasis.contractions import GeneralizedContractionShell as RefShell

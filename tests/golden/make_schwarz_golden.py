@@ -28,7 +28,7 @@ THRESHOLDS = (1e-12, 1e-6, 1e-3)
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="path of a gbasis source checkout")
     a = ap.parse_args()
     sys.path.insert(0, a.reference)
     from gbasis.contractions import GeneralizedContractionShell as RefShell

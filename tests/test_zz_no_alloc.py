@@ -65,3 +65,29 @@ def test_noalloc_rejects_bases_beyond_its_scratch():
     rc = _noalloc(make_workload("medium8"), out)
     assert rc == _engine.GBX_ERR_INVALID
     assert "limited to 64 MiB" in _engine.last_error()
+
+
+def test_noalloc_takes_no_device_memory_and_does_not_wait_for_other_streams():
+    """After a first call (set-up and kernel loading), a call leaves the device's free memory
+    unchanged, and it returns while a bounded kernel queued earlier on another stream is still
+    running: it makes no cudaMalloc/cudaFree and no device-wide synchronisation."""
+    import torch
+    shells = make_workload("tiny4")
+    n = _engine.DeviceBasis(shells).nbf
+    out = torch.empty(n ** 4, dtype=torch.float64, device="cuda")
+    work = torch.cuda.Stream()
+    side = torch.cuda.Stream()
+    sp = ctypes.c_void_p(work.cuda_stream)
+    _engine.check(_noalloc(shells, out, stream=sp), "gbx_eri_full_noalloc")
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    _engine.check(_noalloc(shells, out, stream=sp), "gbx_eri_full_noalloc")
+    work.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    # about a second of spinning on the side stream (2e9 clock cycles: a bounded kernel)
+    with torch.cuda.stream(side):
+        torch.cuda._sleep(2_000_000_000)
+    _engine.check(_noalloc(shells, out, stream=sp), "gbx_eri_full_noalloc")
+    still_running = not side.query()
+    torch.cuda.synchronize()
+    assert still_running, "the call waited for work queued on another stream"
