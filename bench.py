@@ -14,8 +14,8 @@ Cartesian; physicist notation as a view of the chemist array, as gbasis returns 
 * ``cpu_baseline``: the CPU oracle (a NumPy restatement of gbasis's algorithm) on a seeded
   sample of the workload's shell quartets, extrapolated to the whole workload.
 
-``--impl reference`` times that CPU implementation on all host cores instead and prints
-the same metric with ``"impl": "reference"``.  For N > 1 GPUs every rank computes the
+``--impl reference`` times that CPU implementation on all host cores instead (every step a
+measured slice of the workload) and prints the same metric with ``"impl": "reference"``.  For N > 1 GPUs every rank computes the
 same workload (independent replicas: a full-tensor call needs no exchange between GPUs) and
 ``value`` aggregates.
 """
@@ -42,6 +42,7 @@ EXPAND_TRAFFIC_BYTES = 404.778752e6 + 1599.436e6
 
 
 HBM_FALLBACK_GBS = 6650.0  # copy bandwidth measured earlier on a B200 of the same kind
+REF_SLICES = 64  # CPU legs: one step = one interleaved 1/64 slice of the unique shell quartets
 
 
 def _peaks():
@@ -148,6 +149,31 @@ def _cpu_model():
     return platform.machine()
 
 
+def cpu_baseline_slice(shells, n_slices=REF_SLICES, s=0):
+    """The oracle on 1 core over one interleaved 1/``n_slices`` slice of the workload's unique
+    shell quartets (about 11,000 quartets, 10-15 s for medium8): measured unique ERIs over
+    measured time, no extrapolation."""
+    from oracle import eri_oracle as orc
+    from oracle import parallel as opar
+    pairs = opar.unique_pairs(len(shells))
+    nq = opar.quartet_count(len(shells))
+    q = opar.slice_quartets(pairs, nq, s, n_slices)
+    t0 = time.perf_counter()
+    for i, j, k, l in q:
+        blk = orc.construct_array_contraction(shells[i], shells[j], shells[k], shells[l])
+        for ax, x in enumerate((i, j, k, l)):  # norm_cont, as base_four_symm.py:195-205
+            shape = [1] * 8
+            shape[2 * ax:2 * ax + 2] = np.shape(shells[x].norm_cont)
+            blk = blk * np.asarray(shells[x].norm_cont).reshape(shape)
+    dt = time.perf_counter() - t0
+    eris = opar.unique_eri_count(shells, q)
+    return {"value": eris / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "host_cpus": os.cpu_count(), "cpu_model": _cpu_model(),
+            "sample": f"slice {s} of {n_slices} of the {nq} unique shell quartets ({len(q)} "
+                      f"quartets, {eris} unique ERIs, {dt:.1f} s; oracle "
+                      f"construct_array_contraction, 1 core), measured"}
+
+
 def cpu_baseline(shells, seconds=12.0, seed=0, n_functions=None):
     """Oracle on a seeded random sample of unique shell quartets, extrapolated (unique ERIs
     counted over ``n_functions``, default the Cartesian functions)."""
@@ -174,60 +200,59 @@ def cpu_baseline(shells, seconds=12.0, seed=0, n_functions=None):
                       f"oracle construct_array_contraction, 1 core), extrapolated"}
 
 
-def _pool_worker(args):
-    import itertools
-    os.environ.setdefault("OMP_NUM_THREADS", "1")
-    from gbasis_b200.synthetic import make_workload
-    from oracle import eri_oracle as orc
-    seed, seconds = args
-    shells = make_workload(WORKLOAD)
-    pairs = list(itertools.combinations_with_replacement(range(len(shells)), 2))
-    rng = np.random.default_rng(seed)
-    t0 = time.perf_counter()
-    done = 0
-    while time.perf_counter() - t0 < seconds:
-        p, q = sorted(rng.integers(0, len(pairs), size=2))
-        (i, j), (k, l) = pairs[p], pairs[q]
-        orc.construct_array_contraction(shells[i], shells[j], shells[k], shells[l])
-        done += 1
-    return done, time.perf_counter() - t0
+def engine_config(n, nq, n_unique, compact_bytes=None, world=1):
+    """The ``config`` of the headline line, shared by both arms."""
+    cfg = {"workload": WORKLOAD, "n_functions": n, "shell_quartets": nq, "unique_eris": n_unique,
+           "notation": "physicist", "coord_type": "cartesian", "form": "fp64",
+           "parallelism": "replicas" if world > 1 else "single"}
+    if compact_bytes is not None:
+        cfg["l2"] = ("working set above L2 (1.66 GB tensor, "
+                     f"{compact_bytes / 1e6:.0f} MB compact store)")
+    return cfg
 
 
 def run_reference(a, rank, world):
-    """CPU implementation of the path (the oracle port) on all host cores."""
+    """The CPU implementation of the path (the oracle port of gbasis's per-quartet integrals,
+    with gbasis's norm_cont scaling) on every host core.  Each step is measured, not
+    extrapolated: step s computes slice s mod 64 of the workload's unique shell quartets (the
+    quartets at loop positions congruent to s, so every slice has the workload's class mix)
+    over a spawned process pool, and the step's unique ERIs are counted exactly.  ``value``
+    = unique ERIs of the timed steps / their wall time."""
     if rank != 0:
         return
-    import multiprocessing as mp
     from gbasis_b200.synthetic import make_workload
     from gbasis_b200.flops import unique_eris
+    from oracle import parallel as opar
     shells = make_workload(WORKLOAD)
     n = sum(len(s.angmom_components_cart) for s in shells)
-    npair = len(shells) * (len(shells) + 1) // 2
-    nq = npair * (npair + 1) // 2
-    cores = os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    per_step = 4.0
-    vals = []
-    with ctx.Pool(cores) as pool:
+    pairs = opar.unique_pairs(len(shells))
+    nq = opar.quartet_count(len(shells))
+    pool = opar.SlicePool(WORKLOAD)
+    cores = pool.processes
+    times, eris, quartets = [], 0, 0
+    try:
         for step in range(a.warmup + a.steps):
-            res = pool.map(_pool_worker, [(1000 * step + r, per_step) for r in range(cores)])
-            done = sum(d for d, _ in res)
-            wall = max(t for _, t in res)
-            rate_q = done / wall  # quartets per second, all cores
-            v = unique_eris(n) / (nq / rate_q)
+            q = opar.slice_quartets(pairs, nq, step, REF_SLICES)
+            dt = pool.run(q)
             if step >= a.warmup:
-                vals.append(v)
-    v = float(np.mean(vals))
+                times.append(dt)
+                eris += opar.unique_eri_count(shells, q)
+                quartets += len(q)
+    finally:
+        pool.close()
+    total = float(sum(times))
+    v = eris / total
+    cfg = engine_config(n, nq, unique_eris(n), world=world)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": unique_eris(n) / v * 1e3,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": total / len(times) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_functions": n, "shell_quartets": nq,
-                       "notation": "physicist", "coord_type": "cartesian"},
+            "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "cpu_model": _cpu_model(),
-                             "sample": f"{per_step:.0f} s per step per core of random unique "
-                                       f"shell quartets, extrapolated to {nq} quartets"},
+                             "sample": f"{a.steps} timed steps, each one interleaved 1/{REF_SLICES} "
+                                       f"slice of the {nq} unique shell quartets ({quartets} "
+                                       f"quartets, {eris} unique ERIs in all), measured, "
+                                       f"{cores} processes"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -499,16 +524,37 @@ def main():
            "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": 8 * n ** 4, "ms_per_step": e2e_s * 1e3,
            "d2h_copy_floor_ms": d2h_s * 1e3,
-           "d2h_copy_gbs": 8 * n ** 4 / d2h_s / 1e9}
+           "d2h_copy_gbs": 8 * n ** 4 / d2h_s / 1e9,
+           "out": "page-locked array passed as out="}
+    # the default call: no out=, the tensor comes back as a new pageable NumPy array
+    del res
+    t0 = time.perf_counter()
+    for _ in range(max(1, a.e2e_steps)):
+        res = er.electron_repulsion_integral(shells)
+    pg_s = max_over_ranks((time.perf_counter() - t0) / max(1, a.e2e_steps), dist, dev)
+    del res
+    e2e["pageable_default"] = {"value": replica_throughput(world, n_unique, pg_s * 1e3),
+                               "unit": UNIT, "ms_per_step": pg_s * 1e3,
+                               "out": "new pageable array (electron_repulsion_integral(basis))"}
+    # per-quartet drop-in: one construct_array_contraction call (host shells in, NumPy out)
+    cac = {}
+    by_l = {}
+    for sh in shells:
+        by_l.setdefault(sh.angmom, sh)
+    for name, q in (("(ss|ss) K=6", [s for s in shells if s.angmom == 0][0]),
+                    ("(dd|dd)", by_l[2])):
+        quartet = [q] * 4
+        er.ElectronRepulsionIntegral.construct_array_contraction(*quartet)
+        t0 = time.perf_counter()
+        for _ in range(20):
+            er.ElectronRepulsionIntegral.construct_array_contraction(*quartet)
+        cac[name] = (time.perf_counter() - t0) / 20 * 1e3
+    e2e["construct_array_contraction_ms"] = cac
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_functions": n, "shell_quartets": nq,
-                       "unique_eris": n_unique, "notation": "physicist", "coord_type": "cartesian",
-                       "form": "fp64", "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "working set above L2 (1.66 GB tensor, "
-                             f"{compact_bytes / 1e6:.0f} MB compact store)"},
+            "config": engine_config(n, nq, n_unique, compact_bytes, world),
             "phases_ms": {"work_list": ph[0], "class_kernels": ph[1], "expand": ph[2]},
             "roofline": roof, "roofline_kernels": [roof_compute, roof_expand],
             "e2e": e2e, "clocks": clk.summary(), "mixed": mixed,
@@ -524,7 +570,7 @@ def main():
         except Exception as exc:
             line["configs"] = {"error": str(exc)[:300]}
     if rank == 0 and not a.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(shells)
+        line["cpu_baseline"] = cpu_baseline_slice(shells)
     if rank == 0:
         print(json.dumps(line), flush=True)
     db.close()

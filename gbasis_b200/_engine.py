@@ -34,6 +34,7 @@ EXPORTED_SYMBOLS = (
     "gbx_batch_num_types", "gbx_batch_type_info", "gbx_batch_set_team", "gbx_batch_set_profiling",
     "gbx_batch_type_times", "gbx_release_cached_memory", "gbx_eri_jk", "gbx_point_charge",
     "gbx_basis_set_potential", "gbx_batch_run_mixed", "gbx_batch_mixed_counts", "gbx_boys_eval",
+    "gbx_pipe_peak", "gbx_eri_coulomb_j_mixed",
 )
 
 
@@ -79,6 +80,8 @@ def lib():
             "gbx_last_error": [ctypes.c_char_p, ctypes.c_size_t],
             "gbx_fp64_peak": [_I, ctypes.POINTER(_D)],
             "gbx_boys_eval": [_I, _I64, _P, _P],
+            "gbx_pipe_peak": [_I, _I, ctypes.POINTER(_D)],
+            "gbx_eri_coulomb_j_mixed": [_P, _P, _D, _D, _P, _P],
             "gbx_set_profiling": [_P, _I],
             "gbx_phase_times": [_P, _P],
             "gbx_eri_full_noalloc": [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
@@ -405,6 +408,13 @@ def _current_device():
 def fp64_peak(device=0):
     v = ctypes.c_double()
     check(lib().gbx_fp64_peak(int(device), ctypes.byref(v)), "gbx_fp64_peak")
+    return float(v.value)
+
+
+def pipe_peak(pipe, device=0):
+    """Measured TFLOP/s of pipe 0 (FP64 FMA), 1 (FP64 mma.sync) or 2 (FP32 FMA)."""
+    v = ctypes.c_double()
+    check(lib().gbx_pipe_peak(int(device), int(pipe), ctypes.byref(v)), "gbx_pipe_peak")
     return float(v.value)
 
 

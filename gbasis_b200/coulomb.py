@@ -24,10 +24,18 @@ from . import _engine
 __all__ = ["coulomb_matrix", "coulomb_exchange"]
 
 
-def coulomb_matrix(basis, density, schwarz_threshold=1e-12, coord_type=None, device=None):
+def coulomb_matrix(basis, density, schwarz_threshold=1e-12, coord_type=None, device=None,
+                   precision="fp64", mixed_thresholds=None):
     """J (K, K) float64 for the symmetric density ``density`` (K, K) in the basis's
-    functions (coordinate types from the shells unless ``coord_type`` overrides them)."""
+    functions (coordinate types from the shells unless ``coord_type`` overrides them).
+
+    ``precision="mixed"``: quartets are classified by the bound of their final values
+    instead of ``schwarz_threshold``: below ``skip`` left out, below ``fp32`` FP32 recursions
+    (light classes), else FP64; ``mixed_thresholds=(skip, fp32)`` defaults to the mixed
+    full-tensor form's thresholds."""
     import torch
+    if precision not in ("fp64", "mixed"):
+        raise ValueError("`precision` must be 'fp64' or 'mixed'")
     types = None
     if coord_type is not None:
         types = [coord_type] * len(basis) if isinstance(coord_type, str) else list(coord_type)
@@ -41,9 +49,17 @@ def coulomb_matrix(basis, density, schwarz_threshold=1e-12, coord_type=None, dev
         d_D = torch.from_numpy(D).to(dev)
         d_J = torch.empty((n, n), dtype=torch.float64, device=dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
-        _engine.check(_engine.lib().gbx_eri_coulomb_j(
-            db.handle, ctypes.c_void_p(d_D.data_ptr()), float(schwarz_threshold),
-            ctypes.c_void_p(d_J.data_ptr()), ctypes.c_void_p(stream)), "gbx_eri_coulomb_j")
+        if precision == "mixed":
+            from .electron_repulsion import MIXED_FP32, MIXED_SKIP
+            skip, fp32 = mixed_thresholds or (MIXED_SKIP, MIXED_FP32)
+            _engine.check(_engine.lib().gbx_eri_coulomb_j_mixed(
+                db.handle, ctypes.c_void_p(d_D.data_ptr()), float(skip), float(fp32),
+                ctypes.c_void_p(d_J.data_ptr()), ctypes.c_void_p(stream)),
+                "gbx_eri_coulomb_j_mixed")
+        else:
+            _engine.check(_engine.lib().gbx_eri_coulomb_j(
+                db.handle, ctypes.c_void_p(d_D.data_ptr()), float(schwarz_threshold),
+                ctypes.c_void_p(d_J.data_ptr()), ctypes.c_void_p(stream)), "gbx_eri_coulomb_j")
         return d_J.cpu().numpy()
     finally:
         db.close()

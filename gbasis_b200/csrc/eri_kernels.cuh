@@ -233,8 +233,8 @@ __device__ __forceinline__ void coulomb_epilogue(const EriLaunch& a, int2 pq, co
 
 // R = double: the FP64 form.  R = float: the mixed form's FP32 path — Boys values and the
 // geometric factors are formed in FP64 and rounded, the vertical and transfer recursions run
-// in FP32, and each primitive quartet's [e0|f0] is added to FP64 accumulators; the
-// horizontal recursion, transforms and stores stay FP64.
+// in FP32 and [e0|f0] accumulates in FP32 over the lane's primitive quartets; the team
+// reduction, horizontal recursion, transforms and stores are FP64.
 // Resident CTAs per SM a class's register kernel is compiled for.  Classes whose unconstrained
 // register use is 171-200 per thread would fit 2 CTAs of 128 threads per SM; for these the cap
 // of 168 registers that a third CTA needs costs at most a few spilled values, and the extra warps
@@ -259,8 +259,6 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
   constexpr int NCA = ncart(LA), NCB = ncart(LB), NCC = ncart(LC), NCD = ncart(LD);
   __shared__ double s_tab[kBoysNGrid * kBoysTaylor];
   __shared__ double s_exp[kBoysNGrid];
-  stage_boys<L>(a.boys_tab, s_tab, s_exp);
-  __syncthreads();
 
   // A team of `team` consecutive lanes (1..32, power of two) shares one quartet: its lanes
   // take interleaved primitive quartets and the accumulators are summed with shuffles.  The
@@ -271,6 +269,11 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
   const int lane = threadIdx.x & 31;
   const int tl = lane & (team - 1);
   const int per_warp = 32 / team;
+  // a CTA without a quartet (a screened or mixed-form list shorter than the grid) leaves
+  // before staging the Boys table; the test is the same for all its threads
+  if ((long long)blockIdx.x * (blockDim.x >> 5) * per_warp >= count) return;
+  stage_boys<L>(a.boys_tab, s_tab, s_exp);
+  __syncthreads();
   const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long wb = gwarp * per_warp; wb < count; wb += nwarps * per_warp) {
@@ -280,9 +283,9 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
                           : make_int2(0, 0);
     const PairDev P = a.pairs[pq.x];
     const PairDev Q = a.pairs[pq.y];
-    double acc[C::NE * C::NF];
+    R accr[C::NE * C::NF];  // FP32 form: accumulated in FP32 over the primitive quartets
 #pragma unroll
-    for (int i = 0; i < C::NE * C::NF; ++i) acc[i] = 0.0;
+    for (int i = 0; i < C::NE * C::NF; ++i) accr[i] = R(0);
 
     const int nprim = valid ? P.nprim * Q.nprim : 0;
     int ip = tl / Q.nprim, jq = tl - ip * Q.nprim;
@@ -308,20 +311,16 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
         if constexpr (sizeof(R) == sizeof(double)) {
           C::template prim<double>(F, bp.Xx, bp.Xy, bp.Xz, -rz * PQx, -rz * PQy, -rz * PQz,
                                    o2z, rz, fma(ze, bp.Xx, kp.Xx), fma(ze, bp.Xy, kp.Xy),
-                                   fma(ze, bp.Xz, kp.Xz), ze, o2e, acc);
+                                   fma(ze, bp.Xz, kp.Xz), ze, o2e, accr);
         } else {
-          float F32[L + 1], a32[C::NE * C::NF];
+          float F32[L + 1];
 #pragma unroll
           for (int m = 0; m <= L; ++m) F32[m] = (float)F[m];
-#pragma unroll
-          for (int i = 0; i < C::NE * C::NF; ++i) a32[i] = 0.0f;
           C::template prim<float>(F32, (float)bp.Xx, (float)bp.Xy, (float)bp.Xz,
                                   (float)(-rz * PQx), (float)(-rz * PQy), (float)(-rz * PQz),
                                   (float)o2z, (float)rz, (float)fma(ze, bp.Xx, kp.Xx),
                                   (float)fma(ze, bp.Xy, kp.Xy), (float)fma(ze, bp.Xz, kp.Xz),
-                                  (float)ze, (float)o2e, a32);
-#pragma unroll
-          for (int i = 0; i < C::NE * C::NF; ++i) acc[i] += (double)a32[i];
+                                  (float)ze, (float)o2e, accr);
         }
       }
       jq += team;
@@ -330,6 +329,9 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
         ++ip;
       }
     }
+    double acc[C::NE * C::NF];
+#pragma unroll
+    for (int i = 0; i < C::NE * C::NF; ++i) acc[i] = (double)accr[i];
     for (int o = team >> 1; o > 0; o >>= 1) {
 #pragma unroll
       for (int i = 0; i < C::NE * C::NF; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);

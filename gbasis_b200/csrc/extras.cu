@@ -10,7 +10,8 @@
 using namespace gbx;
 
 namespace gbx {
-int coulomb_entry(gbx_basis* b, const double* D, double tau, double* J, cudaStream_t st);
+int coulomb_entry(gbx_basis* b, const double* D, double tau, double* J, cudaStream_t st,
+                  double skip = 0.0, double fp32 = 0.0);
 int jk_entry(gbx_basis* b, const double* D, double tau, double* J, double* K, cudaStream_t st);
 }
 
@@ -39,9 +40,96 @@ __global__ void fp64_fma_probe(double* out, int iters, double a, double b) {
   if (s == 1.2345) out[blockIdx.x] = s;  // keeps the chains live
 }
 
+// FP64 tensor-core rate: 8 independent chains of mma.sync m8n8k4 (512 flops per warp each).
+__global__ void fp64_mma_probe(double* out, int iters, double a, double b) {
+  double c[8][2];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) c[k][0] = c[k][1] = threadIdx.x * 1e-9 + k * 1e-3;
+  const double av = a + threadIdx.x * 1e-12, bv = b;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                     : "+d"(c[k][0]), "+d"(c[k][1])
+                     : "d"(av), "d"(bv));
+    }
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += c[k][0] + c[k][1];
+  if (s == 1.2345) out[blockIdx.x] = s;
+}
+
+// FP32 FMA rate: as fp64_fma_probe in single precision.
+__global__ void fp32_fma_probe(double* out, int iters, float a, float b) {
+  float x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-9f + k * 1e-3f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) x[k] = fmaf(x[k], a, b);
+    }
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == 1.2345f) out[blockIdx.x] = s;
+}
+
 }  // namespace
 
 extern "C" {
+
+int gbx_pipe_peak(int device, int pipe, double* tflops) {
+  if (!tflops || pipe < 0 || pipe > 2)
+    return set_error(GBX_ERR_INVALID, "gbx_pipe_peak: pipe must be 0 (FP64 FMA), 1 (FP64 mma) or 2 (FP32 FMA)");
+  if (pipe == 0) return gbx_fp64_peak(device, tflops);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  double* d = nullptr;
+  int s = cuda_status(cudaMalloc(&d, 4096 * sizeof(double)), "cudaMalloc(probe)");
+  if (s) {
+    cudaSetDevice(prev);
+    return s;
+  }
+  const int blocks = nsm * 8, threads = 256, iters = pipe == 1 ? 1024 : 4096;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto run = [&](int it) {
+    if (pipe == 1) fp64_mma_probe<<<blocks, threads>>>(d, it, 0.999999, 1e-7);
+    else fp32_fma_probe<<<blocks, threads>>>(d, it, 0.999999f, 1e-7f);
+  };
+  run(16);  // warm-up
+  float best = 1e30f;
+  for (int rep = 0; rep < 5; ++rep) {
+    cudaEventRecord(e0);
+    run(iters);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) best = ms;
+  }
+  s = cuda_status(cudaGetLastError(), "pipe probe");
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  cudaSetDevice(prev);
+  if (s) return s;
+  const double warps = (double)blocks * threads / 32;
+  const double flops = pipe == 1 ? 512.0 * 16 * iters * warps                  // 16 mma per iteration
+                                 : 2.0 * 8 * 16 * (double)iters * blocks * threads;
+  *tflops = flops / (best * 1e-3) / 1e12;
+  return GBX_OK;
+}
 
 int gbx_lincomb(const double* in, int64_t n, const double* T, int64_t n_orb, double* out,
                 double* work, void* stream) {
@@ -109,6 +197,14 @@ int gbx_eri_coulomb_j(gbx_basis* b, const double* D, double tau, double* J, void
   if (!b || !D || !J) return set_error(GBX_ERR_INVALID, "gbx_eri_coulomb_j: null argument");
   if (!(tau >= 0.0)) return set_error(GBX_ERR_INVALID, "schwarz threshold must be >= 0");
   return gbx::coulomb_entry(b, D, tau, J, (cudaStream_t)stream);
+}
+
+int gbx_eri_coulomb_j_mixed(gbx_basis* b, const double* D, double skip, double fp32, double* J,
+                            void* stream) {
+  if (!b || !D || !J) return set_error(GBX_ERR_INVALID, "gbx_eri_coulomb_j_mixed: null argument");
+  if (!(skip > 0.0) || !(fp32 >= skip) || !(fp32 < 1.0))
+    return set_error(GBX_ERR_INVALID, "need 0 < skip <= fp32 < 1 (got %g, %g)", skip, fp32);
+  return gbx::coulomb_entry(b, D, 0.0, J, (cudaStream_t)stream, skip, fp32);
 }
 
 int gbx_eri_jk(gbx_basis* b, const double* D, double tau, double* J, double* K, void* stream) {

@@ -341,6 +341,10 @@ __global__ void __launch_bounds__(128, 4) eri_lines(const CoopArgs A) {
   short(*s_ins)[8] = reinterpret_cast<short(*)[8]>(smem);
   short* s_idx = reinterpret_cast<short*>(smem) + 8 * M.n_ins;
   const bool staged = A.prog_doubles > 0;
+  // no quartet for any warp of this CTA: leave before staging (the test is CTA-uniform)
+  if ((long long)blockIdx.x * (blockDim.x >> 5) >=
+      (a.work_count ? (long long)(*a.work_count) : a.nwork))
+    return;
   if (staged) {
     const int4* src = reinterpret_cast<const int4*>(&kCoopIns[M.v_ins][0]);
     int4* dst4 = reinterpret_cast<int4*>(smem);
@@ -557,10 +561,11 @@ __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
   constexpr int NCD = ncart(C::LC) * ncart(C::LD);
   constexpr int RS = split_rs(C::NF, NCD);
   constexpr int QS = C::NE * RS;
+  const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
+  if ((long long)blockIdx.x * 32 >= count) return;  // no quartet for this CTA (uniform)
   stage_boys<L>(a.boys_tab, s_tab, s_exp);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* ACC = dyn;
-  const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
   for (long long base = (long long)blockIdx.x * 32; base < count; base += (long long)gridDim.x * 32) {
     if (threadIdx.x < 32) s_mx[threadIdx.x] = 0ull;
     __syncthreads();  // Boys table staged (first group); previous group's tail done

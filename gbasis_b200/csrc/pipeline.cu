@@ -726,48 +726,82 @@ int launch_diagonal_bounds(const PairDev* pairs, int npairs, const ShellDev* she
 // Bounds of the final values for the mixed form: every output integral satisfies
 // |(ab|cd)| <= sqrt((ab|ab) (cd|cd)) <= Q_p Q_q (Cauchy-Schwarz for the output functions
 // themselves: norm_cont, component norms and spherical transforms included).  The diagonal
-// quartets (p, p) are computed by the class kernels into the compact store (scratch here:
-// the call that follows overwrites it).
+// quartets (p, p) are computed by the class kernels in their store mode, each into its own
+// nf x nf block of a temporary buffer (a copy of the pair records with the pair-function
+// offset 0 and the per-molecule destination index set to the pair), so no compact store is
+// needed: the direct Coulomb path uses these bounds on systems whose store would not fit.
+__global__ void diagonal_block_bounds(const PairDev* __restrict__ pairs, int npairs,
+                                      const ShellDev* __restrict__ shells,
+                                      const long long* __restrict__ off,
+                                      const double* __restrict__ blk, double* __restrict__ q) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const PairDev P = pairs[p];
+  const int nf = shells[P.shA].nout * P.nB;
+  double mx = 0.0;
+  for (int i = 0; i < nf; ++i) mx = fmax(mx, fabs(blk[off[p] + (long long)i * nf + i]));
+  q[p] = sqrt(mx);
+}
+
 static int ensure_mixed_bounds(Basis& B, cudaStream_t st) {
   if (B.mixed_ready) return GBX_OK;
   int s;
   const int np = (int)B.pairs.size();
-  if ((s = B.ensure_scratch(B.compact_elems, 0))) return s;
   if (!B.d_qmixed && (s = B.alloc((void**)&B.d_qmixed, np * sizeof(double), "cudaMalloc(qmixed)")))
     return s;
+  std::vector<PairDev> tp(B.pairs);
   std::vector<int2> diag(np);
-  for (int p = 0; p < np; ++p) diag[p] = make_int2(p, p);
-  int2* d_diag = nullptr;
-  GBX_CUDA(cudaMalloc(&d_diag, np * sizeof(int2)), "cudaMalloc(diagonal quartets)");
-  cudaError_t e = cudaMemcpyAsync(d_diag, diag.data(), np * sizeof(int2), cudaMemcpyHostToDevice, st);
+  std::vector<long long> off(np + 1, 0), ncols(np);
+  for (int p = 0; p < np; ++p) {
+    const long long nf = (long long)B.shells[tp[p].shA].nout * tp[p].nB;
+    tp[p].fo = 0;
+    tp[p].mol = p;
+    diag[p] = make_int2(p, p);
+    ncols[p] = nf;
+    off[p + 1] = off[p] + nf * nf;
+  }
+  const size_t bytes = np * (sizeof(PairDev) + sizeof(int2) + 2 * sizeof(long long)) +
+                       (size_t)off[np] * sizeof(double);
+  unsigned char* tmp = nullptr;
+  GBX_CUDA(cudaMalloc(&tmp, bytes), "cudaMalloc(diagonal quartets)");
+  PairDev* d_tp = reinterpret_cast<PairDev*>(tmp);
+  int2* d_diag = reinterpret_cast<int2*>(d_tp + np);
+  long long* d_off = reinterpret_cast<long long*>(d_diag + np);
+  long long* d_ncols = d_off + np;
+  double* d_blk = reinterpret_cast<double*>(d_ncols + np);
+  cudaError_t e = cudaMemcpyAsync(d_tp, tp.data(), np * sizeof(PairDev), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_diag, diag.data(), np * sizeof(int2), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_off, off.data(), np * sizeof(long long), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_ncols, ncols.data(), np * sizeof(long long), cudaMemcpyHostToDevice, st);
   const int nsm = num_sms(B.device);
-  for (int c = 0; c < kNumPairClasses && e == cudaSuccess; ++c) {
+  s = GBX_OK;
+  for (int c = 0; c < kNumPairClasses && e == cudaSuccess && !s; ++c) {
     if (B.class_count[c] == 0) continue;
-    const BlockDev& bd = B.block_table[(size_t)c * kNumPairClasses + c];
     EriLaunch a = base_launch(B);
+    a.pairs = d_tp;
     a.work = d_diag;
     a.work_off = B.class_first[c];
     a.nwork = B.class_count[c];
-    a.base = bd.base;
-    a.ncols = bd.ncols;
+    a.out = d_blk;
+    a.mol_base = d_off;
+    a.mol_ncols = d_ncols;
     a.mode = 0;
     a.team = 1;
     const int grid = (int)std::min<long long>((a.nwork + 127) / 128, (long long)nsm * 8);
     s = launch_class(kPairClassL[c][0], kPairClassL[c][1], kPairClassL[c][0], kPairClassL[c][1],
                      a, std::max(grid, 1), st);
-    if (s) {
-      cudaStreamSynchronize(st);
-      cudaFree(d_diag);
-      return s;
-    }
   }
-  if (e == cudaSuccess) {
-    diagonal_bounds<<<(np + 127) / 128, 128, 0, st>>>(B.d_pairs, np, B.d_shells, B.d_blocks,
-                                                      B.d_compact, B.d_qmixed);
+  if (e == cudaSuccess && !s) {
+    diagonal_block_bounds<<<(np + 127) / 128, 128, 0, st>>>(d_tp, np, B.d_shells, d_off, d_blk,
+                                                            B.d_qmixed);
     e = cudaGetLastError();
   }
   const cudaError_t e2 = cudaStreamSynchronize(st);
-  cudaFree(d_diag);
+  cudaFree(tmp);
+  if (s) return s;
   GBX_CUDA(e, "mixed-form bounds");
   GBX_CUDA(e2, "mixed-form bounds");
   B.mixed_ready = true;
@@ -858,40 +892,180 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
   return GBX_OK;
 }
 
-// Direct Coulomb matrix: the unique quartets of every class block, in chunks of
-// kCoulombChunk candidates (Schwarz-screened and compacted by build_work_range), feed the
-// class kernels in mode 2, which accumulate J with atomics.  No integral is stored.
-int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st) {
-  int s;
-  if (tau > 0.0 && (s = ensure_schwarz(B, st))) return s;
-  const long long chunk = kCoulombChunk;
-  if (!B.d_jwork) {
-    if ((s = B.alloc((void**)&B.d_jwork, (size_t)chunk * sizeof(int2), "cudaMalloc(J work)")))
-      return s;
+// Direct Coulomb matrix.  Within each pair class the pairs are ordered by their bound,
+// largest first, so that for a bra pair the ket pairs that pass the screening form a prefix of
+// its class's order (and, in the mixed form, the FP64 quartets a prefix of that prefix).  The
+// host counts every row's quartets by binary search; the device expands row ranges of those
+// counts into work lists chunk by chunk (expand_jwork) and the class kernels contract each
+// chunk with D as it is produced (mode 2, atomics into J).  Work is proportional to the
+// quartets that survive, not to the N_pair^2 candidates; class blocks run concurrently on the
+// basis's auxiliary streams, each stream with its own work buffer.  No integral is stored.
+__global__ void expand_jwork(const long long* __restrict__ row_start, int nrows,
+                             const int* __restrict__ first_col, const int* __restrict__ perm_b,
+                             const int* __restrict__ perm_k, long long w0, long long len,
+                             int2* __restrict__ work) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= len) return;
+  const long long w = w0 + t;
+  int lo = 0, hi = nrows - 1;  // the last row whose start is <= w (it is not empty)
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (row_start[mid] <= w) lo = mid;
+    else hi = mid - 1;
   }
-  GBX_CUDA(cudaMemsetAsync(J, 0, (size_t)B.nbf * B.nbf * sizeof(double), st), "clear J");
-  const int nsm = num_sms(B.device);
-  const int nblk = (int)B.blocks.size();
-  long long computed = 0;
-  for (int i = 0; i < nblk; ++i) {
-    const int k = B.launch_order.empty() ? i : B.launch_order[i];
+  work[t] = make_int2(perm_b[lo], perm_k[first_col[lo] + (int)(w - row_start[lo])]);
+}
+
+namespace {
+// number of entries of the descending array k[0..n) that are >= x
+inline long long count_ge(const double* k, long long n, double x) {
+  return std::upper_bound(k, k + n, x, [](double v, double e) { return v > e; }) - k;
+}
+}  // namespace
+
+int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st, double skip,
+                double fp32) {
+  int s;
+  const bool mixed = skip > 0.0 || fp32 > 0.0;
+  if (mixed && B.potential)
+    return set_error(GBX_ERR_UNSUPPORTED, "the mixed-precision form computes 1/r integrals only");
+  if ((s = ensure_schwarz(B, st))) return s;
+  const int np = (int)B.pairs.size();
+  std::vector<double> key(np);
+  if (mixed) {
+    if ((s = ensure_mixed_bounds(B, st))) return s;
+    GBX_CUDA(cudaMemcpy(key.data(), B.d_qmixed, np * sizeof(double), cudaMemcpyDeviceToHost),
+             "download final-value bounds");
+  } else {
+    key = B.h_q;
+  }
+  // per class: pairs by descending bound
+  std::vector<int> perm(np);
+  std::vector<double> ks(np);
+  for (int c = 0; c < kNumPairClasses; ++c) {
+    const long long f = B.class_first[c], n = B.class_count[c];
+    for (long long i = 0; i < n; ++i) perm[f + i] = (int)(f + i);
+    std::stable_sort(perm.begin() + f, perm.begin() + f + n,
+                     [&](int x, int y) { return key[x] > key[y]; });
+    for (long long i = 0; i < n; ++i) ks[f + i] = key[perm[f + i]];
+  }
+  // per class block and precision: row starts and first ket positions
+  struct JList {
+    int blk, fp32;
+    long long total;
+    size_t row_off, col_off;  // into rows / cols
+    int nrows;
+  };
+  std::vector<JList> lists;
+  std::vector<long long> rows;
+  std::vector<int> cols;
+  long long computed = 0, candidates = 0;
+  const double lo64 = mixed ? std::max(fp32, skip) : tau;  // FP64 when the bound is >= lo64
+  const double lo = mixed ? skip : tau;                     // computed when the bound is >= lo
+  for (int k = 0; k < (int)B.blocks.size(); ++k) {
     const HostBlock& h = B.blocks[k];
-    const BuildBlock bb{(int)B.class_first[h.cb], (int)h.nb, (int)B.class_first[h.ck], (int)h.nk,
-                        h.tri ? 1 : 0, k, 0, h.ncand};
-    for (long long start = 0; start < h.ncand; start += chunk) {
-      const long long len = std::min(chunk, h.ncand - start);
-      int* cnt = B.d_counts + k;
-      GBX_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), st), "clear chunk count");
-      build_work_range<<<(int)((len + 255) / 256), 256, 0, st>>>(bb, start, len, B.d_qscreen, tau,
-                                                                 B.d_jwork, cnt);
-      GBX_CUDA(cudaGetLastError(), "build_work_range launch");
+    candidates += h.ncand;
+    const long long fb = B.class_first[h.cb], nb = B.class_count[h.cb];
+    const long long fk = B.class_first[h.ck], nk = B.class_count[h.ck];
+    const bool has32 = mixed && block_has_fp32(h);
+    for (int prec = 0; prec < (has32 ? 2 : 1); ++prec) {
+      JList L{k, prec, 0, rows.size(), cols.size(), (int)nb};
+      rows.push_back(0);
+      for (long long i = 0; i < nb; ++i) {
+        const double kb = ks[fb + i];
+        auto upto = [&](double cut) -> long long {
+          if (cut <= 0.0) return nk;
+          if (!(kb > 0.0)) return 0;
+          return count_ge(ks.data() + fk, nk, cut / kb);
+        };
+        long long n_all = upto(lo), n64 = has32 ? upto(lo64) : n_all;
+        if (h.tri) {
+          n_all = std::min(n_all, i + 1);
+          n64 = std::min(n64, i + 1);
+        }
+        const long long first = prec == 0 ? 0 : n64;
+        const long long cnt = prec == 0 ? n64 : n_all - n64;
+        cols.push_back((int)first);
+        rows.push_back(rows.back() + std::max<long long>(cnt, 0));
+      }
+      L.total = rows.back();
+      computed += L.total;
+      if (L.total > 0) lists.push_back(L);
+    }
+  }
+  B.last_computed = computed;
+  B.last_screened = candidates - computed;
+  GBX_CUDA(cudaMemsetAsync(J, 0, (size_t)B.nbf * B.nbf * sizeof(double), st), "clear J");
+  if (lists.empty()) return GBX_OK;
+  // device copies (one block, kept by the basis until the next call)
+  const size_t bytes = np * sizeof(int) + rows.size() * sizeof(long long) + cols.size() * sizeof(int);
+  if (B.jplan_bytes < bytes) {
+    if (B.d_jplan) B.release(B.d_jplan);
+    B.d_jplan = nullptr;
+    if ((s = B.alloc(&B.d_jplan, bytes, "cudaMalloc(J plan)"))) return s;
+    B.jplan_bytes = bytes;
+  }
+  long long* d_rows = reinterpret_cast<long long*>(B.d_jplan);
+  int* d_perm = reinterpret_cast<int*>(d_rows + rows.size());
+  int* d_cols = d_perm + np;
+  GBX_CUDA(cudaMemcpyAsync(d_rows, rows.data(), rows.size() * sizeof(long long),
+                           cudaMemcpyHostToDevice, st), "upload J rows");
+  GBX_CUDA(cudaMemcpyAsync(d_perm, perm.data(), np * sizeof(int), cudaMemcpyHostToDevice, st),
+           "upload J order");
+  GBX_CUDA(cudaMemcpyAsync(d_cols, cols.data(), cols.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           st), "upload J columns");
+  // the host vectors are pageable: the copies above have completed on return
+  const int nstreams = kAuxStreams;
+  if (B.aux.empty()) {
+    B.aux.resize(nstreams);
+    B.join.resize(nstreams);
+    for (int j = 0; j < nstreams; ++j) {
+      GBX_CUDA(cudaStreamCreateWithFlags(&B.aux[j], cudaStreamNonBlocking), "create stream");
+      GBX_CUDA(cudaEventCreateWithFlags(&B.join[j], cudaEventDisableTiming), "create event");
+    }
+    GBX_CUDA(cudaEventCreateWithFlags(&B.fork, cudaEventDisableTiming), "create event");
+  }
+  long long biggest = 0;
+  for (const JList& L : lists) biggest = std::max(biggest, L.total);
+  const long long chunk = std::min<long long>(kCoulombChunk, biggest);
+  if (!B.d_jwork || B.jwork_cap < chunk * nstreams) {
+    if (B.d_jwork) B.release(B.d_jwork);
+    B.d_jwork = nullptr;
+    if ((s = B.alloc((void**)&B.d_jwork, (size_t)chunk * nstreams * sizeof(int2), "cudaMalloc(J work)")))
+      return s;
+    B.jwork_cap = chunk * nstreams;
+  }
+  GBX_CUDA(cudaEventRecord(B.fork, st), "fork");
+  for (int j = 0; j < nstreams; ++j) GBX_CUDA(cudaStreamWaitEvent(B.aux[j], B.fork, 0), "fork wait");
+  // largest lists first, round robin over the streams
+  std::vector<int> order(lists.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    const HostBlock& hx = B.blocks[lists[x].blk];
+    const HostBlock& hy = B.blocks[lists[y].blk];
+    return lists[x].total * hx.avg_prims > lists[y].total * hy.avg_prims;
+  });
+  const int nsm = num_sms(B.device);
+  for (size_t oi = 0; oi < order.size(); ++oi) {
+    const JList& L = lists[order[oi]];
+    const int j = (int)(oi % nstreams);
+    const cudaStream_t bs = B.aux[j];
+    int2* wk = B.d_jwork + (size_t)j * chunk;
+    const HostBlock& h = B.blocks[L.blk];
+    for (long long w0 = 0; w0 < L.total; w0 += chunk) {
+      const long long len = std::min(chunk, L.total - w0);
+      expand_jwork<<<(int)((len + 255) / 256), 256, 0, bs>>>(
+          d_rows + L.row_off, L.nrows, d_cols + L.col_off, d_perm + B.class_first[h.cb],
+          d_perm + B.class_first[h.ck], w0, len, wk);
+      GBX_CUDA(cudaGetLastError(), "expand_jwork launch");
       EriLaunch a = base_launch(B);
-      a.work = B.d_jwork;
-      a.work_count = cnt;
+      a.work = wk;
+      a.work_count = nullptr;
       a.work_off = 0;
       a.nwork = len;
       a.mode = 2;
       a.team = h.team;
+      a.fp32 = L.fp32;
       a.potential = B.potential;
       a.omega = B.omega;
       a.D = D;
@@ -900,12 +1074,14 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
       const int grid =
           (int)std::max<long long>(1, std::min<long long>((len * h.team + 127) / 128, (long long)nsm * 8));
       if ((s = launch_class(kPairClassL[h.cb][0], kPairClassL[h.cb][1], kPairClassL[h.ck][0],
-                            kPairClassL[h.ck][1], a, grid, st)))
+                            kPairClassL[h.ck][1], a, grid, bs)))
         return s;
-      computed += len;
     }
   }
-  (void)computed;
+  for (int j = 0; j < nstreams; ++j) {
+    GBX_CUDA(cudaEventRecord(B.join[j], B.aux[j]), "join");
+    GBX_CUDA(cudaStreamWaitEvent(st, B.join[j], 0), "join wait");
+  }
   return GBX_OK;
 }
 

@@ -435,10 +435,11 @@ struct gbx_basis {
 };
 
 namespace gbx {
-int coulomb_entry(gbx_basis* b, const double* D, double tau, double* J, cudaStream_t st) {
+int coulomb_entry(gbx_basis* b, const double* D, double tau, double* J, cudaStream_t st,
+                  double skip, double fp32) {
   Basis& B = *b->impl;
   DeviceGuard g(B.device);
-  return run_coulomb(B, D, tau, J, st);
+  return run_coulomb(B, D, tau, J, st, skip, fp32);
 }
 int jk_entry(gbx_basis* b, const double* D, double tau, double* J, double* K, cudaStream_t st) {
   Basis& B = *b->impl;

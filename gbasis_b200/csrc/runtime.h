@@ -12,7 +12,7 @@
 namespace gbx {
 
 constexpr int kAuxStreams = 6;
-constexpr long long kCoulombChunk = 1LL << 24;  // quartet candidates per Coulomb chunk
+constexpr long long kCoulombChunk = 1LL << 23;  // quartets per direct-Coulomb work chunk
 constexpr int kStageBuffers = 3;                // host-output staging slabs in flight
 constexpr size_t kStageBytes = 64ull << 20;     // target bytes of one staging slab
 
@@ -47,7 +47,10 @@ struct Basis {
   std::vector<int4> h_rowinfo;
   int* d_gtab = nullptr;
   int4* d_rowinfo = nullptr;
-  int2* d_jwork = nullptr;  // Coulomb chunk work list
+  int2* d_jwork = nullptr;  // direct Coulomb: one work-chunk buffer per auxiliary stream
+  long long jwork_cap = 0;
+  void* d_jplan = nullptr;   // direct Coulomb: row starts, pair order, first ket positions
+  size_t jplan_bytes = 0;
   int* d_counts32 = nullptr;   // mixed form: FP32 quartets per block
   double* d_qmixed = nullptr;  // mixed form: per-pair bound of the final values
   std::vector<long long> class_first, class_count, class_funcs;
@@ -120,7 +123,8 @@ int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, d
              double fp32 = 0.0);
 int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStream_t st);
 int run_compact(Basis& B, double tau, cudaStream_t st, double skip = 0.0, double fp32 = 0.0);
-int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st);
+int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st,
+                double skip = 0.0, double fp32 = 0.0);
 int run_jk(Basis& B, const double* D, double tau, double* J, double* K, cudaStream_t st);
 int run_point_charge(Basis& B, int npoints, const double* coords, const double* charges,
                      int sum, double* out, cudaStream_t st);

@@ -197,9 +197,19 @@ int gbx_batch_mixed_counts(const gbx_batch* b, int64_t* n_fp64, int64_t* n_fp32,
                            int64_t* n_skipped);
 
 /* Coulomb matrix J[a,b] = sum_cd (ab|cd) D[c,d] from the screened unique quartets
- * (full tensor never stored).  D, J: device N x N row-major (D symmetric). */
+ * (full tensor never stored; only quartets with Q_p Q_q >= schwarz_threshold are enumerated,
+ * Q the bounds of compute_schwarz_bounds).  D, J: device N x N row-major (D symmetric).
+ * gbx_last_counts: quartets computed and screened out. */
 int gbx_eri_coulomb_j(gbx_basis* b, const double* D, double schwarz_threshold, double* J,
                       void* stream);
+
+/* Mixed-precision direct Coulomb matrix: quartets whose final-value bound (Q_p Q_q over the
+ * output functions, norm_cont and transforms included) is below `skip` are left out, those
+ * below `fp32` in light classes run their recursions in FP32, the rest in FP64; the
+ * contraction with D and J stay FP64.  0 < skip <= fp32 < 1.  Same replacement as
+ * gbx_eri_coulomb_j (no direct counterpart in gbasis). */
+int gbx_eri_coulomb_j_mixed(gbx_basis* b, const double* D, double skip, double fp32, double* J,
+                            void* stream);
 
 /* Coulomb and exchange matrices of a density D (any N x N, not only symmetric):
  *   J[a,b] = sum_cd (ab|cd) D[c,d],   K[a,c] = sum_bd (ab|cd) D[b,d]   (chemist notation),
@@ -251,6 +261,13 @@ int gbx_last_error(char* buf, size_t len);
 
 /* Sustained FP64 FMA rate of the device (TFLOP/s) from a dependent-FMA microbenchmark. */
 int gbx_fp64_peak(int device, double* tflops);
+
+/* Measured rate (TFLOP/s) of one arithmetic pipe of the device: pipe 0 = FP64 FMA (as
+ * gbx_fp64_peak), 1 = FP64 tensor-core mma.sync m8n8k4, 2 = FP32 FMA.  The roofline
+ * denominators of the FP64 and FP32 recursions, and the evidence for or against FP64 tensor
+ * cores for the small dense contractions (HRR, spherical transform).  No reference
+ * counterpart (gbasis has no device code). */
+int gbx_pipe_peak(int device, int pipe, double* tflops);
 
 /* Boys values F_0..F_{m_max}(T[i]) on the current device, computed by the same device
  * function the class kernels use (Taylor table for T < 40, asymptotic form above), for

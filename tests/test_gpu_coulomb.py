@@ -125,3 +125,47 @@ def test_jk_rejects_bad_arguments():
                                        D.data_ptr(), None))
     finally:
         db.close()
+
+
+def test_direct_coulomb_large64_subset_against_oracle_rows():
+    """The 64-atom box's first 16 atoms (160 spherical shells with f, N = 480): direct J
+    without screening against J rows assembled from oracle blocks, J_ab = sum_cd (ab|cd) D_cd
+    over every ket shell pair (both orders of an off-diagonal ket pair, D symmetric), for bra
+    shell pairs s(8)s(8), p-d and f-f on different atoms.  The screened J (1e-12) and the mixed
+    form's J stay within 1e-10 of it."""
+    import os
+    from oracle import parallel as opar
+    wl = "large64:160"
+    shells = opar.workload_shells(wl)
+    sizes = [2 * s.angmom + 1 if s.coord_type in ("spherical", "p") else
+             len(s.angmom_components_cart) for s in shells]
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    n = int(off[-1])
+    assert n == 480
+    D = density_matrix(n)
+    J = coulomb_matrix(shells, D, schwarz_threshold=0.0)
+    byl = {}
+    for x, s in enumerate(shells):
+        byl.setdefault((s.angmom, len(s.exps)), []).append(x)
+    bra = [(byl[(0, 8)][0], byl[(0, 8)][3]), (byl[(1, 3)][1], byl[(2, 2)][5]),
+           (byl[(3, 1)][2], byl[(3, 1)][9])]
+    kets = [(k, l) for k in range(len(shells)) for l in range(k, len(shells))]
+    quart = np.array([(i, j, k, l) for i, j in bra for k, l in kets])
+    vals = opar.oracle_blocks(wl, quart, processes=min(os.cpu_count() or 1, 32), chunk=64)
+    pos = 0
+    scale = max(1.0, float(np.abs(J).max()))
+    for i, j in bra:
+        ref = np.zeros((sizes[i], sizes[j]))
+        for k, l in kets:
+            m = sizes[i] * sizes[j] * sizes[k] * sizes[l]
+            blk = vals[pos:pos + m].reshape(sizes[i], sizes[j], sizes[k], sizes[l])
+            pos += m
+            dcd = D[off[k]:off[k + 1], off[l]:off[l + 1]]
+            ref += (1.0 if k == l else 2.0) * np.einsum("abcd,cd->ab", blk, dcd)
+        got = J[off[i]:off[i + 1], off[j]:off[j + 1]]
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-12 * scale)
+    assert pos == vals.size
+    Jt = coulomb_matrix(shells, D, schwarz_threshold=1e-12)
+    assert np.abs(Jt - J).max() <= 1e-10
+    Jm = coulomb_matrix(shells, D, precision="mixed")
+    assert np.abs(Jm - J).max() <= 1e-10
