@@ -266,12 +266,13 @@ def extra_configs(local, reps=2):
       with the mixed form's max error over the whole compact store;
     * ``batch512``: 512 molecules of 2-14 atoms, one CUDA graph per run (every molecule's full
       Cartesian tensor, device resident), FP64 and mixed form side by side;
-    * ``large64_coulomb_subset``: direct Coulomb matrix of the first 16 atoms of the 64-atom
-      box (160 spherical shells, N = 480; the full 64-atom system takes minutes).
+    * ``large64_coulomb``: direct Coulomb matrix of the 64-atom box (640 spherical shells,
+      N = 1920), FP64 and mixed form, with the screened fraction and the mixed J's error.
     """
     import ctypes
     import torch
     from gbasis_b200 import _engine
+    from gbasis_b200.autotune import light_class
     from gbasis_b200.batch import EriBatch
     from gbasis_b200.electron_repulsion import MIXED_FP32, MIXED_SKIP
     from gbasis_b200.flops import basis_flops, unique_eris
@@ -281,16 +282,17 @@ def extra_configs(local, reps=2):
     sp = ctypes.c_void_p(st.cuda_stream)
     peak64 = _engine.fp64_peak(local)
 
-    def timed(fn):
+    def timed(fn, n=None):
+        n = reps if n is None else n
         fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
-        for _ in range(reps):
+        for _ in range(n):
             fn()
         e1.record(st)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / reps
+        return e0.elapsed_time(e1) / n
 
     out = {}
     shells = make_workload("chain20")
@@ -337,6 +339,19 @@ def extra_configs(local, reps=2):
         "value": uq / (ms * 1e-3), "unit": UNIT, "molecules_per_s": len(mols) / (ms * 1e-3),
         "achieved_tflops": fl / (ms * 1e-3) / 1e12, "frac_fp64_peak": fl / (ms * 1e-3) / 1e12 / peak64,
         "create_s": t_create, "launch": "one CUDA graph replay per run"}
+    try:  # the same block types one after another with events between them (no overlap)
+        Lb = _engine.lib()
+        _engine.check(Lb.gbx_batch_set_profiling(b.handle, 1))
+        b.run(outs, stream=sp)
+        torch.cuda.synchronize()
+        tms = np.zeros(len(b.types()))
+        _engine.check(Lb.gbx_batch_type_times(b.handle, tms.ctypes.data_as(ctypes.c_void_p), len(tms)))
+        _engine.check(Lb.gbx_batch_set_profiling(b.handle, 0))
+        out["batch512"]["types_serial_ms"] = float(tms.sum())
+        out["batch512"]["heavy_types_serial_ms"] = float(sum(
+            t for (c4, _, _, _), t in zip(b.types(), tms) if not light_class(c4)))
+    except Exception as exc:
+        out["batch512"]["types_serial_ms"] = {"error": str(exc)[:200]}
     # mixed form of the same batch, side by side (its own graph); error against the FP64
     # tensors of every 8th molecule with N <= 80
     try:
@@ -363,21 +378,43 @@ def extra_configs(local, reps=2):
     del outs
     torch.cuda.empty_cache()
 
-    shells = make_workload("large64")[:160]
+    # config 5: the full 64-atom box, direct J only (the unique integrals would take 13.6 TB)
+    shells = make_workload("large64")
+    t0 = time.perf_counter()
     db = _engine.DeviceBasis(shells, device=local)
+    t_create = time.perf_counter() - t0
     n = db.nbf
     D = torch.from_numpy(density_matrix(n)).to(dev)
     J = torch.empty((n, n), dtype=torch.float64, device=dev)
+    Jm = torch.empty((n, n), dtype=torch.float64, device=dev)
+    L = _engine.lib()
+    tau = 1e-12
 
     def coulomb():
-        _engine.check(_engine.lib().gbx_eri_coulomb_j(
-            db.handle, ctypes.c_void_p(D.data_ptr()), 1e-12, ctypes.c_void_p(J.data_ptr()), sp),
-            "gbx_eri_coulomb_j")
-    ms = timed(coulomb)
-    nq = db.stats()[0]
-    out["large64_coulomb_subset"] = {
-        "atoms": 16, "n_functions": n, "shell_quartets": nq, "schwarz_threshold": 1e-12,
-        "ms": ms, "quartets_per_s": nq / (ms * 1e-3), "unit": "shell quartets/s (before screening)"}
+        _engine.check(L.gbx_eri_coulomb_j(db.handle, ctypes.c_void_p(D.data_ptr()), tau,
+                                          ctypes.c_void_p(J.data_ptr()), sp), "gbx_eri_coulomb_j")
+
+    def coulomb_mixed():
+        _engine.check(L.gbx_eri_coulomb_j_mixed(
+            db.handle, ctypes.c_void_p(D.data_ptr()), MIXED_SKIP, MIXED_FP32,
+            ctypes.c_void_p(Jm.data_ptr()), sp), "gbx_eri_coulomb_j_mixed")
+    ms = timed(coulomb, 1)
+    computed, screened = db.last_counts()
+    ms_mx = timed(coulomb_mixed, 1)
+    computed_mx, skipped_mx = db.last_counts()
+    dj = float((Jm - J).abs().max())
+    out["large64_coulomb"] = {
+        "atoms": 64, "shells": len(shells), "n_functions": n, "coord_type": "spherical",
+        "candidate_quartets": computed + screened, "schwarz_threshold": tau,
+        "fp64": {"ms": ms, "quartets_computed": computed,
+                 "screened_fraction": screened / max(1, computed + screened),
+                 "quartets_per_s": computed / (ms * 1e-3),
+                 "unit": "screened unique shell quartets/s"},
+        "mixed": {"ms": ms_mx, "quartets_computed": computed_mx,
+                  "quartets_per_s": computed_mx / (ms_mx * 1e-3), "speedup_vs_fp64": ms / ms_mx,
+                  "max_abs_J_err_vs_fp64": dj, "max_abs_J": float(J.abs().max()),
+                  "skip_bound": MIXED_SKIP, "fp32_bound": MIXED_FP32},
+        "density": "D = X X^T / ||X X^T||, X seeded normal N x N/4", "create_s": t_create}
     db.close()
     torch.cuda.empty_cache()
     return out

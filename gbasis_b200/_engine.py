@@ -34,7 +34,8 @@ EXPORTED_SYMBOLS = (
     "gbx_batch_num_types", "gbx_batch_type_info", "gbx_batch_set_team", "gbx_batch_set_profiling",
     "gbx_batch_type_times", "gbx_release_cached_memory", "gbx_eri_jk", "gbx_point_charge",
     "gbx_basis_set_potential", "gbx_batch_run_mixed", "gbx_batch_mixed_counts", "gbx_boys_eval",
-    "gbx_pipe_peak", "gbx_eri_coulomb_j_mixed",
+    "gbx_pipe_peak", "gbx_eri_coulomb_j_mixed", "gbx_set_block_config", "gbx_basis_set_streams",
+    "gbx_batch_set_type_config",
 )
 
 
@@ -82,6 +83,9 @@ def lib():
             "gbx_boys_eval": [_I, _I64, _P, _P],
             "gbx_pipe_peak": [_I, _I, ctypes.POINTER(_D)],
             "gbx_eri_coulomb_j_mixed": [_P, _P, _D, _D, _P, _P],
+            "gbx_set_block_config": [_P, _I, _I, _I],
+            "gbx_basis_set_streams": [_P, _I],
+            "gbx_batch_set_type_config": [_P, _I, _I, _I],
             "gbx_set_profiling": [_P, _I],
             "gbx_phase_times": [_P, _P],
             "gbx_eri_full_noalloc": [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P],
@@ -360,6 +364,13 @@ class DeviceBasis:
 
     def set_team(self, k, team):
         check(lib().gbx_set_team(self.handle, int(k), int(team)), "gbx_set_team")
+
+    def set_block_config(self, k, variant=0, ctas_per_sm=8):
+        check(lib().gbx_set_block_config(self.handle, int(k), int(variant), int(ctas_per_sm)),
+              "gbx_set_block_config")
+
+    def set_streams(self, n):
+        check(lib().gbx_basis_set_streams(self.handle, int(n)), "gbx_basis_set_streams")
 
     def block_times(self):
         n = ctypes.c_int()

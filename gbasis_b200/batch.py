@@ -73,39 +73,76 @@ class EriBatch:
         table = _load() if table is None else table
         n = 0
         for k, (cls4, team, avg, _) in enumerate(self.types()):
-            t = table.get(_key(cls4, avg))
+            key = _key(cls4, avg)
+            t = table.get(key)
             if t and t != team:
                 self.set_team(k, int(t))
                 n += 1
+            v, c = table.get("v:" + key), table.get("c:" + key)
+            if v is not None or c is not None:
+                self.set_type_config(k, int(v or 0), int(c or 8))
+                n += 1
         return n
 
+    def set_type_config(self, k, variant=0, ctas_per_sm=8):
+        _engine.check(_engine.lib().gbx_batch_set_type_config(self.handle, int(k), int(variant),
+                                                              int(ctas_per_sm)),
+                      "gbx_batch_set_type_config")
+
     def autotune(self, outs, teams=None, reps=2, save=True, stream=None):
-        """Time every register-kernel block type with each team (types run one after another,
-        CUDA events per type), keep the fastest, store the choices in the tuning cache."""
+        """Time every block type with each value of its knobs (types run one after another,
+        CUDA events per type): the team of the register-kernel types, then the kernel variant
+        of the heavy types, then the grid cap of the register-kernel types; keep the fastest
+        and store the choices in the tuning cache."""
         import json
-        from .autotune import TEAMS, _key, _load, cache_path, light_class
+        from .autotune import CTAS, TEAMS, _key, _load, cache_path, light_class
         teams = TEAMS if teams is None else teams
         L = _engine.lib()
         types = self.types()
+        keys = [_key(c4, avg) for c4, _, avg, _ in types]
         light = [k for k, (c4, _, _, _) in enumerate(types) if light_class(c4)]
-        times = np.full((len(teams), len(types)), np.inf)
-        _engine.check(L.gbx_batch_set_profiling(self.handle, 1))
-        try:
-            for ti, t in enumerate(teams):
-                for k in light:
-                    self.set_team(k, t)
+        heavy = [k for k in range(len(types)) if k not in light]
+        var = {k: 0 for k in range(len(types))}
+        cap = {k: 8 for k in range(len(types))}
+
+        def sweep(ks, values, setter):
+            times = np.full((len(values), len(types)), np.inf)
+            for vi, v in enumerate(values):
+                for k in ks:
+                    setter(k, v)
                 for _ in range(reps):
                     self.run(outs, stream=stream)
                     ms = np.zeros(len(types))
                     _engine.check(L.gbx_batch_type_times(self.handle, _engine._ptr(ms), len(ms)))
-                    times[ti] = np.minimum(times[ti], ms)
+                    times[vi] = np.minimum(times[vi], ms)
+            return times
+
+        def set_var(k, v):
+            var[k] = v
+            self.set_type_config(k, v, cap[k])
+
+        def set_cap(k, c):
+            cap[k] = c
+            self.set_type_config(k, var[k], c)
+        chosen = {}
+        _engine.check(L.gbx_batch_set_profiling(self.handle, 1))
+        try:
+            times = sweep(light, teams, self.set_team)
+            for k in light:
+                best = teams[int(np.argmin(times[:, k]))]
+                self.set_team(k, best)
+                chosen[keys[k]] = best
+            t_var = sweep(heavy, (0, 1), set_var)
+            for k in heavy:
+                set_var(k, int(np.argmin(t_var[:, k])))
+                chosen["v:" + keys[k]] = var[k]
+            t_cap = sweep(light, CTAS, set_cap)
+            for k in light:
+                set_cap(k, CTAS[int(np.argmin(t_cap[:, k]))])
+                chosen["c:" + keys[k]] = cap[k]
         finally:
             _engine.check(L.gbx_batch_set_profiling(self.handle, 0))
-        chosen = {}
-        for k in light:
-            best = teams[int(np.argmin(times[:, k]))]
-            self.set_team(k, best)
-            chosen[_key(types[k][0], types[k][2])] = best
+        times = {"team": times, "variant": t_var, "ctas_per_sm": t_cap}
         if save:
             table = _load()
             table.update(chosen)

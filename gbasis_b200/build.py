@@ -49,7 +49,8 @@ HOST_DEPS = ("gbx_common.cuh", "runtime.h", "errors.h", "pipeline_kernels.cuh", 
              "coop_tail.cuh", "_gen/coop_programs.cuh")
 
 
-LINES_DEPS = ("gbx_common.cuh", "errors.h", "coop.cuh", "coop_tail.cuh", "lines_kernel.cuh")
+LINES_DEPS = ("gbx_common.cuh", "errors.h", "coop.cuh", "coop_tail.cuh", "lines_kernel.cuh",
+              "eri_kernels.cuh", "_gen/eri_gen.cuh")
 
 
 def _deps_mtime(src):

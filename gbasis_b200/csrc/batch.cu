@@ -34,6 +34,8 @@ struct BatchType {
   long long n = 0, work_off = 0;
   double avg_prims = 1.0;
   int team = 1;
+  int variant = 0;      // heavy classes with both kernels: 0 split, 1 line kernel
+  int ctas_per_sm = 8;  // grid cap of the register kernel (resident-CTA multiples of the SMs)
   long long* d_base = nullptr;   // per molecule: block base in the batch compact store
   long long* d_ncols = nullptr;  // per molecule: pair functions of the ket class
 };
@@ -478,6 +480,7 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st, bool mixed = false) {
     a.nwork = T.n;
     a.mode = 0;
     a.team = T.team;
+    a.variant = T.variant;
     a.mol_base = T.d_base;
     a.mol_ncols = T.d_ncols;
     cudaStream_t ts = Bt.profile ? st : Bt.aux[i % Bt.aux.size()];
@@ -488,7 +491,7 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st, bool mixed = false) {
     }
     if (a.nwork > 0) {
       const int grid = (int)std::max<long long>(
-          1, std::min<long long>((a.nwork * T.team + 127) / 128, (long long)nsm * 8));
+          1, std::min<long long>((a.nwork * T.team + 127) / 128, (long long)nsm * T.ctas_per_sm));
       int s = launch_class(kPairClassL[T.cb][0], kPairClassL[T.cb][1], kPairClassL[T.ck][0],
                            kPairClassL[T.ck][1], a, grid, ts);
       if (s) return s;
@@ -498,7 +501,7 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st, bool mixed = false) {
       a.nwork = Bt.mix_n32[k];
       a.fp32 = 1;
       const int grid = (int)std::max<long long>(
-          1, std::min<long long>((a.nwork * T.team + 127) / 128, (long long)nsm * 8));
+          1, std::min<long long>((a.nwork * T.team + 127) / 128, (long long)nsm * T.ctas_per_sm));
       int s = launch_class(kPairClassL[T.cb][0], kPairClassL[T.cb][1], kPairClassL[T.ck][0],
                            kPairClassL[T.ck][1], a, grid, ts);
       if (s) return s;
@@ -646,6 +649,22 @@ int gbx_batch_type_info(const gbx_batch* b, int k, int* cls4, int* team, double*
   if (team) *team = T.team;
   if (avg_prims) *avg_prims = T.avg_prims;
   if (n_quartets) *n_quartets = T.n;
+  return GBX_OK;
+}
+
+int gbx_batch_set_type_config(gbx_batch* b, int k, int variant, int ctas_per_sm) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_batch_set_type_config: null batch");
+  Batch& B = *b->impl;
+  if (k < 0 || k >= (int)B.types.size()) return set_error(GBX_ERR_INVALID, "type %d out of range", k);
+  if (variant < 0 || variant > 1) return set_error(GBX_ERR_INVALID, "variant must be 0 or 1");
+  if (ctas_per_sm < 1 || ctas_per_sm > 32)
+    return set_error(GBX_ERR_INVALID, "ctas_per_sm must be in [1, 32]");
+  BatchType& T = B.types[k];
+  if (T.variant != variant || T.ctas_per_sm != ctas_per_sm) {
+    T.variant = variant;
+    T.ctas_per_sm = ctas_per_sm;
+    batch_drop_graph(B);
+  }
   return GBX_OK;
 }
 

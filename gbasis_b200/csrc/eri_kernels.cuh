@@ -249,6 +249,11 @@ __host__ __device__ constexpr int eri_min_blocks(int la, int lb, int lc, int ld)
              : 1;
 }
 
+// Classes whose quartet holds at most 16 accumulators are bound by the per-primitive-quartet
+// Boys evaluation, not by their recursions: their lanes take two primitive quartets per step.
+template <int NACC>
+constexpr bool kEriPairPrims = NACC <= 16;
+
 // ATT: the instantiation for the range-separated operators (a.potential != 0); the 1/r kernels
 // carry no attenuation code.
 template <int LA, int LB, int LC, int LD, typename R, bool ATT = false>
@@ -289,44 +294,64 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
 
     const int nprim = valid ? P.nprim * Q.nprim : 0;
     int ip = tl / Q.nprim, jq = tl - ip * Q.nprim;
-    for (int idx = tl; idx < nprim; idx += team) {
-      {
-        const PrimPair bp = a.prims[P.prim_off + ip];
-        const double o2z = 0.5 * bp.izeta;
-        const PrimPair kp = a.prims[Q.prim_off + jq];
-        const double r = rsqrt(bp.zeta + kp.zeta);
-        const double inv = r * r;
-        const double PQx = bp.Px - kp.Px, PQy = bp.Py - kp.Py, PQz = bp.Pz - kp.Pz;
-        const double rz = kp.zeta * inv;  // rho / zeta
-        const double T = bp.zeta * rz * fma(PQx, PQx, fma(PQy, PQy, PQz * PQz));
-        double F[L + 1];
-        boys_eval<L>(T, s_tab, s_exp, F);
-        if constexpr (ATT)
-          boys_attenuate<L>(a.potential, a.omega, bp.zeta * rz, T, s_tab, s_exp, F);
-        const double pref = bp.C * kp.C * r;
+    // one primitive quartet (bra primitive pair ip, ket jq) with weight w (0 or 1) into accr
+    auto prim_quartet = [&](int ipx, int jqx, double w) {
+      const PrimPair bp = a.prims[P.prim_off + ipx];
+      const double o2z = 0.5 * bp.izeta;
+      const PrimPair kp = a.prims[Q.prim_off + jqx];
+      const double r = rsqrt(bp.zeta + kp.zeta);
+      const double inv = r * r;
+      const double PQx = bp.Px - kp.Px, PQy = bp.Py - kp.Py, PQz = bp.Pz - kp.Pz;
+      const double rz = kp.zeta * inv;  // rho / zeta
+      const double T = bp.zeta * rz * fma(PQx, PQx, fma(PQy, PQy, PQz * PQz));
+      double F[L + 1];
+      boys_eval<L>(T, s_tab, s_exp, F);
+      if constexpr (ATT)
+        boys_attenuate<L>(a.potential, a.omega, bp.zeta * rz, T, s_tab, s_exp, F);
+      const double pref = bp.C * kp.C * r * w;
 #pragma unroll
-        for (int m = 0; m <= L; ++m) F[m] *= pref;
-        const double ze = bp.zeta * kp.izeta;
-        const double o2e = 0.5 * kp.izeta;
-        if constexpr (sizeof(R) == sizeof(double)) {
-          C::template prim<double>(F, bp.Xx, bp.Xy, bp.Xz, -rz * PQx, -rz * PQy, -rz * PQz,
-                                   o2z, rz, fma(ze, bp.Xx, kp.Xx), fma(ze, bp.Xy, kp.Xy),
-                                   fma(ze, bp.Xz, kp.Xz), ze, o2e, accr);
-        } else {
-          float F32[L + 1];
+      for (int m = 0; m <= L; ++m) F[m] *= pref;
+      const double ze = bp.zeta * kp.izeta;
+      const double o2e = 0.5 * kp.izeta;
+      if constexpr (sizeof(R) == sizeof(double)) {
+        C::template prim<double>(F, bp.Xx, bp.Xy, bp.Xz, -rz * PQx, -rz * PQy, -rz * PQz, o2z,
+                                 rz, fma(ze, bp.Xx, kp.Xx), fma(ze, bp.Xy, kp.Xy),
+                                 fma(ze, bp.Xz, kp.Xz), ze, o2e, accr);
+      } else {
+        float F32[L + 1];
 #pragma unroll
-          for (int m = 0; m <= L; ++m) F32[m] = (float)F[m];
-          C::template prim<float>(F32, (float)bp.Xx, (float)bp.Xy, (float)bp.Xz,
-                                  (float)(-rz * PQx), (float)(-rz * PQy), (float)(-rz * PQz),
-                                  (float)o2z, (float)rz, (float)fma(ze, bp.Xx, kp.Xx),
-                                  (float)fma(ze, bp.Xy, kp.Xy), (float)fma(ze, bp.Xz, kp.Xz),
-                                  (float)ze, (float)o2e, accr);
-        }
+        for (int m = 0; m <= L; ++m) F32[m] = (float)F[m];
+        C::template prim<float>(F32, (float)bp.Xx, (float)bp.Xy, (float)bp.Xz,
+                                (float)(-rz * PQx), (float)(-rz * PQy), (float)(-rz * PQz),
+                                (float)o2z, (float)rz, (float)fma(ze, bp.Xx, kp.Xx),
+                                (float)fma(ze, bp.Xy, kp.Xy), (float)fma(ze, bp.Xz, kp.Xz),
+                                (float)ze, (float)o2e, accr);
       }
+    };
+    auto advance = [&]() {
       jq += team;
       while (jq >= Q.nprim) {
         jq -= Q.nprim;
         ++ip;
+      }
+    };
+    if constexpr (kEriPairPrims<C::NE * C::NF>) {
+      // Boys-bound classes (few accumulators): two primitive quartets per step, so that each
+      // lane has two independent Boys evaluations in flight; an odd last one is paired with a
+      // repeat of itself at weight 0
+      for (int idx = tl; idx < nprim; idx += 2 * team) {
+        const int ipa = ip, jqa = jq;
+        advance();
+        const bool second = idx + team < nprim;
+        const int ipb = second ? ip : ipa, jqb = second ? jq : jqa;
+        advance();
+        prim_quartet(ipa, jqa, 1.0);
+        prim_quartet(ipb, jqb, second ? 1.0 : 0.0);
+      }
+    } else {
+      for (int idx = tl; idx < nprim; idx += team) {
+        prim_quartet(ip, jq, 1.0);
+        advance();
       }
     }
     double acc[C::NE * C::NF];

@@ -97,6 +97,8 @@ struct EriLaunch {
   // two-electron operator: 0 = 1/r, 1 = erf(omega r)/r, 2 = erfc(omega r)/r
   int potential;
   double omega;
+  // heavy classes that have both kernels: 0 = split register kernel, 1 = line kernel
+  int variant;
 };
 
 // Destination block of a quartet whose bra pair is P.

@@ -808,6 +808,20 @@ static int ensure_mixed_bounds(Basis& B, cudaStream_t st) {
   return GBX_OK;
 }
 
+// The basis's auxiliary streams (kMaxAuxStreams, made on first use; calls use the first
+// B.n_streams of them) with their join events and the fork event.
+static int ensure_aux_streams(Basis& B) {
+  if (!B.aux.empty()) return GBX_OK;
+  B.aux.assign(kMaxAuxStreams, nullptr);
+  B.join.assign(kMaxAuxStreams, nullptr);
+  for (int j = 0; j < kMaxAuxStreams; ++j) {
+    GBX_CUDA(cudaStreamCreateWithFlags(&B.aux[j], cudaStreamNonBlocking), "create stream");
+    GBX_CUDA(cudaEventCreateWithFlags(&B.join[j], cudaEventDisableTiming), "create event");
+  }
+  GBX_CUDA(cudaEventCreateWithFlags(&B.fork, cudaEventDisableTiming), "create event");
+  return GBX_OK;
+}
+
 int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32) {
   int s;
   const bool mixed = skip > 0.0 || fp32 > 0.0;
@@ -839,17 +853,9 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
   // first) so that small and latency-bound classes overlap; per-block timing runs them in
   // order on the caller's stream instead.
   const bool per_block = B.profiling && B.profile_level >= 2;
-  const int nstreams = per_block ? 0 : kAuxStreams;
+  const int nstreams = per_block ? 0 : B.n_streams;
   if (nstreams) {
-    if (B.aux.empty()) {
-      B.aux.resize(nstreams);
-      B.join.resize(nstreams);
-      for (int j = 0; j < nstreams; ++j) {
-        GBX_CUDA(cudaStreamCreateWithFlags(&B.aux[j], cudaStreamNonBlocking), "create stream");
-        GBX_CUDA(cudaEventCreateWithFlags(&B.join[j], cudaEventDisableTiming), "create event");
-      }
-      GBX_CUDA(cudaEventCreateWithFlags(&B.fork, cudaEventDisableTiming), "create event");
-    }
+    if ((s = ensure_aux_streams(B))) return s;
     GBX_CUDA(cudaEventRecord(B.fork, st), "fork");
     for (int j = 0; j < nstreams; ++j) GBX_CUDA(cudaStreamWaitEvent(B.aux[j], B.fork, 0), "fork wait");
   }
@@ -869,10 +875,11 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
     a.ncols = h.dev.ncols;
     a.mode = 0;
     a.team = h.team;
+    a.variant = h.variant;
     a.potential = B.potential;
     a.omega = B.omega;
-    const int grid =
-        (int)std::max<long long>(1, std::min<long long>((h.ncand * h.team + 127) / 128, (long long)nsm * 8));
+    const int grid = (int)std::max<long long>(
+        1, std::min<long long>((h.ncand * h.team + 127) / 128, (long long)nsm * h.ctas_per_sm));
     if (per_block) cudaEventRecord(B.blk_ev[i], st);
     if ((s = launch_class(la, lb, lc, ld, a, grid, bs))) return s;
     if (mixed && block_has_fp32(h)) {  // the block's FP32 list
@@ -1015,16 +1022,8 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
   GBX_CUDA(cudaMemcpyAsync(d_cols, cols.data(), cols.size() * sizeof(int), cudaMemcpyHostToDevice,
                            st), "upload J columns");
   // the host vectors are pageable: the copies above have completed on return
-  const int nstreams = kAuxStreams;
-  if (B.aux.empty()) {
-    B.aux.resize(nstreams);
-    B.join.resize(nstreams);
-    for (int j = 0; j < nstreams; ++j) {
-      GBX_CUDA(cudaStreamCreateWithFlags(&B.aux[j], cudaStreamNonBlocking), "create stream");
-      GBX_CUDA(cudaEventCreateWithFlags(&B.join[j], cudaEventDisableTiming), "create event");
-    }
-    GBX_CUDA(cudaEventCreateWithFlags(&B.fork, cudaEventDisableTiming), "create event");
-  }
+  const int nstreams = B.n_streams;
+  if ((s = ensure_aux_streams(B))) return s;
   long long biggest = 0;
   for (const JList& L : lists) biggest = std::max(biggest, L.total);
   const long long chunk = std::min<long long>(kCoulombChunk, biggest);
@@ -1065,14 +1064,15 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
       a.nwork = len;
       a.mode = 2;
       a.team = h.team;
+      a.variant = h.variant;
       a.fp32 = L.fp32;
       a.potential = B.potential;
       a.omega = B.omega;
       a.D = D;
       a.J = J;
       a.nbf = B.nbf;
-      const int grid =
-          (int)std::max<long long>(1, std::min<long long>((len * h.team + 127) / 128, (long long)nsm * 8));
+      const int grid = (int)std::max<long long>(
+          1, std::min<long long>((len * h.team + 127) / 128, (long long)nsm * h.ctas_per_sm));
       if ((s = launch_class(kPairClassL[h.cb][0], kPairClassL[h.cb][1], kPairClassL[h.ck][0],
                             kPairClassL[h.ck][1], a, grid, bs)))
         return s;

@@ -666,6 +666,26 @@ int gbx_set_team(gbx_basis* b, int k, int team) {
   return GBX_OK;
 }
 
+int gbx_set_block_config(gbx_basis* b, int k, int variant, int ctas_per_sm) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_set_block_config: null basis");
+  Basis& B = *b->impl;
+  if (k < 0 || k >= (int)B.blocks.size()) return set_error(GBX_ERR_INVALID, "block %d out of range", k);
+  if (variant < 0 || variant > 1) return set_error(GBX_ERR_INVALID, "variant must be 0 or 1");
+  if (ctas_per_sm < 1 || ctas_per_sm > 32)
+    return set_error(GBX_ERR_INVALID, "ctas_per_sm must be in [1, 32]");
+  B.blocks[k].variant = variant;
+  B.blocks[k].ctas_per_sm = ctas_per_sm;
+  return GBX_OK;
+}
+
+int gbx_basis_set_streams(gbx_basis* b, int n_streams) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_basis_set_streams: null basis");
+  if (n_streams < 1 || n_streams > kMaxAuxStreams)
+    return set_error(GBX_ERR_INVALID, "n_streams must be in [1, %d]", kMaxAuxStreams);
+  b->impl->n_streams = n_streams;
+  return GBX_OK;
+}
+
 int gbx_block_times(gbx_basis* b, double* ms, int n) {
   if (!b || !ms) return set_error(GBX_ERR_INVALID, "gbx_block_times: null argument");
   Basis& B = *b->impl;

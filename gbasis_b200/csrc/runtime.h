@@ -11,7 +11,8 @@
 
 namespace gbx {
 
-constexpr int kAuxStreams = 6;
+constexpr int kAuxStreams = 6;      // default concurrent class-block streams of a basis
+constexpr int kMaxAuxStreams = 16;  // the most a basis may be given
 constexpr long long kCoulombChunk = 1LL << 23;  // quartets per direct-Coulomb work chunk
 constexpr int kStageBuffers = 3;                // host-output staging slabs in flight
 constexpr size_t kStageBytes = 64ull << 20;     // target bytes of one staging slab
@@ -26,6 +27,8 @@ struct HostBlock {
   BlockDev dev;
   double avg_prims = 1.0;  // mean primitive quartets per shell quartet
   int team = 1;            // lanes per quartet (register kernel), set by heuristic or autotuner
+  int variant = 0;         // heavy classes with both kernels: 0 split, 1 line kernel
+  int ctas_per_sm = 8;     // grid cap of the register kernel: resident-CTA multiples of the SMs
 };
 
 struct Basis {
@@ -93,6 +96,7 @@ struct Basis {
   int profile_level = 0;
   std::vector<int> launch_order;    // class blocks, largest estimated cost first
   std::vector<cudaStream_t> aux;    // concurrent class-block streams
+  int n_streams = kAuxStreams;      // how many of them the class blocks are spread over
   std::vector<cudaEvent_t> join;
   cudaEvent_t fork = nullptr;
   // host-output streaming: staging slabs on the device, copied out on their own stream

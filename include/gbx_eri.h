@@ -182,6 +182,8 @@ int gbx_batch_num_types(const gbx_batch* b, int* n);
 int gbx_batch_type_info(const gbx_batch* b, int k, int* cls4, int* team, double* avg_prims,
                         int64_t* n_quartets);
 int gbx_batch_set_team(gbx_batch* b, int k, int team);
+/* The same knobs per block type of a batch (changing them drops the captured graph). */
+int gbx_batch_set_type_config(gbx_batch* b, int k, int variant, int ctas_per_sm);
 int gbx_batch_set_profiling(gbx_batch* b, int on);
 int gbx_batch_type_times(gbx_batch* b, double* ms, int n);
 /* Mixed-precision form of gbx_batch_run (the batched counterpart of gbx_eri_full_mixed; no
@@ -238,6 +240,13 @@ int gbx_num_blocks(const gbx_basis* b, int* n);
 int gbx_block_info(const gbx_basis* b, int k, int* cls4, int* team, double* avg_prims,
                    int64_t* n_quartets);
 int gbx_set_team(gbx_basis* b, int k, int team);
+/* Further launch knobs of block k (the autotuner's): variant 0 runs a heavy class that has
+ * both kernels on the split register kernel, 1 on the line kernel (no effect on other
+ * classes); ctas_per_sm (1..32) caps the register kernel's grid at that many CTAs per SM.
+ * gbx_basis_set_streams: number of concurrent streams (1..16, default 6) the class blocks of
+ * a call are spread over.  No reference counterpart (gbasis runs one quartet at a time). */
+int gbx_set_block_config(gbx_basis* b, int k, int variant, int ctas_per_sm);
+int gbx_basis_set_streams(gbx_basis* b, int n_streams);
 int gbx_block_times(gbx_basis* b, double* ms, int n);
 
 /* Point-charge interaction integrals of the basis's functions (the replacement of

@@ -66,8 +66,11 @@ def unique_eri_count(shells, quartets):
 
 
 def workload_shells(workload):
-    """The shells of a named synthetic workload; ``"name:n"`` takes its first n shells."""
-    from gbasis_b200.synthetic import make_workload
+    """The shells of a named synthetic workload; ``"name:n"`` takes its first n shells and
+    ``"batch512@m"`` is molecule m of the batch."""
+    from gbasis_b200.synthetic import batch_molecule, make_workload
+    if workload.startswith("batch512@"):
+        return batch_molecule(int(workload.split("@", 1)[1]))
     name, _, n = workload.partition(":")
     shells = make_workload(name)
     return shells[: int(n)] if n else shells

@@ -100,7 +100,9 @@ def test_batch_autotuner_keeps_values():
     torch.cuda.synchronize()
     ref = [o.clone() for o in outs]
     chosen, times = b.autotune(outs, teams=(1, 4, 32), reps=1, save=False)
-    assert chosen and np.isfinite(times).any()
+    assert chosen and set(times) == {"team", "variant", "ctas_per_sm"}
+    assert np.isfinite(times["team"]).any() and np.isfinite(times["ctas_per_sm"]).any()
+    assert any(k.startswith("v:") for k in chosen) and any(k.startswith("c:") for k in chosen)
     for k, (c4, team, avg, nq) in enumerate(b.types()):
         assert team in (1, 2, 4, 8, 16, 32)
     b.run(outs)
@@ -160,3 +162,68 @@ def test_batch_mixed_form_against_fp64_and_single_path():
                                              mixed_skip=th[0], mixed_fp32=th[1])
     for o, ref in zip(outs, o64[:2]):
         assert float((o - ref).abs().max()) <= 1e-10
+
+
+def test_single_basis_autotuner_knobs_keep_values():
+    """Team, kernel variant, grid cap and stream count tuned on a small basis with d shells
+    (heavy classes with both kernels); the tensor is unchanged up to the order of the
+    primitive sums."""
+    import torch
+    from gbasis_b200 import _engine, autotune
+    from gbasis_b200.synthetic import make_workload
+    shells = make_workload("medium8")[:24]
+    db = _engine.DeviceBasis(shells, tuned=False)
+    n = db.nbf
+    ref = torch.empty(n ** 4, dtype=torch.float64, device="cuda")
+    db.full_device(ref.data_ptr())
+    chosen, timings = autotune.autotune(shells, reps=1, teams=(1, 8), ctas=(4, 8),
+                                        streams=(1, 6), save=False)
+    assert chosen["streams"] in (1, 6)
+    assert set(timings) == {"team", "variant", "ctas_per_sm", "streams"}
+    got = torch.empty_like(ref)
+    autotune.apply_cache(db, chosen)
+    db.full_device(got.data_ptr())
+    torch.cuda.synchronize()
+    assert float((got - ref).abs().max()) <= 1e-13
+    db.close()
+
+
+def test_batch_heavily_contracted_quartets_against_oracle():
+    """The batch's three largest molecules (d shells with up to 6 primitives, so up to
+    6^4 = 1296 primitive quartets per shell quartet): 160 seeded (dd|dd) shell quartets whose
+    four d shells have at least 4 primitives each, plus 60 other quartets with a d shell, from
+    the batch's own tensors against the oracle at 1e-12."""
+    import os
+    import torch
+    from oracle import parallel as opar
+    sizes = {m: sum(len(s.angmom_components_cart) for s in batch_molecule(m)) for m in range(512)}
+    big = sorted(sizes, key=lambda m: -sizes[m])[:3]
+    mols = [batch_molecule(m) for m in big]
+    b = EriBatch(mols)
+    outs = [torch.empty((n,) * 4, dtype=torch.float64, device="cuda") for n in b.nbf]
+    b.run(outs)
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(11)
+    for m, shells, out in zip(big, mols, outs):
+        T = out.cpu().numpy()
+        nf = np.array([len(s.angmom_components_cart) for s in shells])
+        off = np.concatenate([[0], np.cumsum(nf)])
+        pairs = opar.unique_pairs(len(shells))
+        allq = opar.quartet_at(pairs, np.arange(opar.quartet_count(len(shells))))
+        l = np.array([s.angmom for s in shells])[allq]
+        k = np.array([len(s.exps) for s in shells])[allq]
+        heavy = np.nonzero((l == 2).all(axis=1) & (k >= 4).all(axis=1))[0]
+        other = np.nonzero((l == 2).any(axis=1))[0]
+        pick = np.union1d(rng.choice(heavy, size=min(160, len(heavy)), replace=False),
+                          rng.choice(other, size=min(60, len(other)), replace=False))
+        q = allq[pick]
+        ref = opar.oracle_blocks(f"batch512@{m}", q, processes=min(os.cpu_count() or 1, 16),
+                                 chunk=4)
+        pos = 0
+        for i, j, kk, ll in q:
+            blk = T[off[i]:off[i + 1], off[j]:off[j + 1], off[kk]:off[kk + 1], off[ll]:off[ll + 1]]
+            r = ref[pos:pos + blk.size].reshape(blk.shape)
+            pos += blk.size
+            np.testing.assert_allclose(blk, r, rtol=0, atol=ATOL)
+        assert pos == ref.size
+    b.close()
