@@ -24,13 +24,18 @@ struct CoopArgs {
 constexpr long long kCoopMaxSmem = 227 * 1024;
 
 // Shared-memory plan of a cooperative launch.  Per warp: ACC (NE*NF) followed by the larger
-// of phase A's `phase_a` doubles and the tail's buffers (rows R and columns Cc per HRR chunk,
-// halved until a warp fits 48 KB); the class's programs are staged once per CTA when they fit;
-// up to 4 warps per CTA.
-inline int coop_plan(const CoopMeta& M, long long phase_a, CoopArgs& A, size_t& smem, int& wpc) {
+// of phase A's `phase_a` doubles and the tail's buffers (rows R and columns Cc per HRR chunk);
+// the class's programs are staged once per CTA when they fit 32 KB; 1 to 4 warps per CTA.
+// Among the chunk sizes R, Cc in {8, 4, 2, 1}, staging or not, and 1..4 warps per CTA, the plan
+// keeps the one with the most warps resident per SM (228 KB of shared memory per SM, 1 KB of it
+// reserved per CTA; at most `max_warps_regs` warps by registers), then the larger chunks, then
+// staged programs: shared memory, not registers, is what limits these kernels' occupancy (a
+// class with f shells took 125 KB per 4-warp CTA with the largest chunks: 4 warps per SM).
+inline int coop_plan(const CoopMeta& M, long long phase_a, CoopArgs& A, size_t& smem, int& wpc,
+                     int max_warps_regs = 16) {
   const int NCD = ncart(M.lc) * ncart(M.ld), NAB = ncart(M.la) * ncart(M.lb);
   const int NENF = M.NE * M.NF;
-  const long long budget = 48 * 1024 / 8;
+  const long long warp_cap = 48 * 1024 / 8;
   auto size_for = [&](int R, int Cc) {
     long long s = NENF + phase_a;
     s = std::max<long long>(s, NENF + (long long)M.NE * NCD + (long long)R * M.nK);
@@ -39,26 +44,40 @@ inline int coop_plan(const CoopMeta& M, long long phase_a, CoopArgs& A, size_t& 
                                    2 * NAB);
     return s;
   };
-  int R = 8, Cc = 8;
-  while ((R > 1 || Cc > 1) && size_for(R, Cc) > budget) {
-    if (R > 1) R /= 2;
-    if (Cc > 1) Cc /= 2;
-  }
-  A.R = R;
-  A.Cc = Cc;
-  const long long per_warp = size_for(R, Cc);
-  A.smem_per_warp = (int)per_warp;
   const long long prog_bytes = (long long)M.n_ins * 16 + (long long)M.n_idx * 2;
   const long long extra = (long long)A.extra_doubles * 8;
-  A.prog_doubles = 0;
-  if (prog_bytes <= 32 * 1024 && prog_bytes + extra + per_warp * 8 <= kCoopMaxSmem)
-    A.prog_doubles = (int)((prog_bytes + 15) / 16 * 2);
-  const long long avail = kCoopMaxSmem - (long long)A.prog_doubles * 8 - extra;
-  wpc = (int)std::max<long long>(1, std::min<long long>(4, avail / (per_warp * 8)));
-  smem = (size_t)A.prog_doubles * 8 + (size_t)extra + (size_t)wpc * per_warp * 8;
-  if ((long long)smem > kCoopMaxSmem)
-    return set_error(GBX_ERR_UNSUPPORTED, "class (%d%d|%d%d) needs %zu bytes of shared memory",
-                     M.la, M.lb, M.lc, M.ld, smem);
+  const long long sm_bytes = 228 * 1024, reserved = 1024;
+  long long best_key = -1;
+  for (int R = 8; R >= 1; R /= 2)
+    for (int Cc = 8; Cc >= 1; Cc /= 2) {
+      const long long per_warp = size_for(R, Cc);
+      if (per_warp > warp_cap && !(R == 1 && Cc == 1)) continue;
+      for (int staged = 1; staged >= 0; --staged) {
+        if (staged && prog_bytes > 32 * 1024) continue;
+        const long long prog = staged ? (prog_bytes + 15) / 16 * 16 : 0;
+        for (int w = 1; w <= 4; ++w) {
+          const long long cta = prog + extra + (long long)w * per_warp * 8;
+          if (cta > kCoopMaxSmem) continue;
+          const long long ctas = std::min<long long>(sm_bytes / (cta + reserved),
+                                                     std::max(1, max_warps_regs / w));
+          const long long warps = ctas * w;
+          // most resident warps, then larger chunks, then staged programs, then fewer warps
+          const long long key = ((warps * 128 + R * Cc) * 2 + staged) * 8 + (4 - w);
+          if (warps > 0 && key > best_key) {
+            best_key = key;
+            A.R = R;
+            A.Cc = Cc;
+            A.smem_per_warp = (int)per_warp;
+            A.prog_doubles = staged ? (int)(prog / 8) : 0;
+            wpc = w;
+            smem = (size_t)cta;
+          }
+        }
+      }
+    }
+  if (best_key < 0)
+    return set_error(GBX_ERR_UNSUPPORTED, "class (%d%d|%d%d) does not fit the shared memory",
+                     M.la, M.lb, M.lc, M.ld);
   return GBX_OK;
 }
 

@@ -249,11 +249,6 @@ __host__ __device__ constexpr int eri_min_blocks(int la, int lb, int lc, int ld)
              : 1;
 }
 
-// Classes whose quartet holds at most 16 accumulators are bound by the per-primitive-quartet
-// Boys evaluation, not by their recursions: their lanes take two primitive quartets per step.
-template <int NACC>
-constexpr bool kEriPairPrims = NACC <= 16;
-
 // ATT: the instantiation for the range-separated operators (a.potential != 0); the 1/r kernels
 // carry no attenuation code.
 template <int LA, int LB, int LC, int LD, typename R, bool ATT = false>
@@ -294,7 +289,7 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
 
     const int nprim = valid ? P.nprim * Q.nprim : 0;
     int ip = tl / Q.nprim, jq = tl - ip * Q.nprim;
-    // one primitive quartet (bra primitive pair ip, ket jq) with weight w (0 or 1) into accr
+    // one primitive quartet (bra primitive pair ipx, ket jqx) with weight w into accr
     auto prim_quartet = [&](int ipx, int jqx, double w) {
       const PrimPair bp = a.prims[P.prim_off + ipx];
       const double o2z = 0.5 * bp.izeta;
@@ -335,24 +330,9 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
         ++ip;
       }
     };
-    if constexpr (kEriPairPrims<C::NE * C::NF>) {
-      // Boys-bound classes (few accumulators): two primitive quartets per step, so that each
-      // lane has two independent Boys evaluations in flight; an odd last one is paired with a
-      // repeat of itself at weight 0
-      for (int idx = tl; idx < nprim; idx += 2 * team) {
-        const int ipa = ip, jqa = jq;
-        advance();
-        const bool second = idx + team < nprim;
-        const int ipb = second ? ip : ipa, jqb = second ? jq : jqa;
-        advance();
-        prim_quartet(ipa, jqa, 1.0);
-        prim_quartet(ipb, jqb, second ? 1.0 : 0.0);
-      }
-    } else {
-      for (int idx = tl; idx < nprim; idx += team) {
-        prim_quartet(ip, jq, 1.0);
-        advance();
-      }
+    for (int idx = tl; idx < nprim; idx += team) {
+      prim_quartet(ip, jq, 1.0);
+      advance();
     }
     double acc[C::NE * C::NF];
 #pragma unroll

@@ -822,6 +822,61 @@ static int ensure_aux_streams(Basis& B) {
   return GBX_OK;
 }
 
+namespace {
+// number of entries of the descending array k[0..n) that are >= x
+inline long long count_ge(const double* k, long long n, double x) {
+  return std::upper_bound(k, k + n, x, [](double v, double e) { return v > e; }) - k;
+}
+}  // namespace
+
+// Mixed form: per class block, upper bounds of its FP32 and left-out quartet counts, counted
+// on the host from the final-value bounds ordered per class (a pair of pairs is below a
+// threshold when the product of their bounds is; thresholds moved by 1e-9 relative in the
+// direction that makes each count an upper bound of the device's classification).  Used to skip the FP32 launch of
+// blocks without FP32 quartets, to size launch grids, and to clear the compact store only when
+// quartets are left out.  Recomputed when the thresholds change.
+static int ensure_mixed_counts(Basis& B, double skip, double fp32) {
+  if (B.mix_key_skip == skip && B.mix_key_fp32 == fp32 && !B.mix_n32.empty()) return GBX_OK;
+  const int np = (int)B.pairs.size();
+  std::vector<double> q(np);
+  GBX_CUDA(cudaMemcpy(q.data(), B.d_qmixed, np * sizeof(double), cudaMemcpyDeviceToHost),
+           "download final-value bounds");
+  std::vector<double> ks(np);
+  for (int c = 0; c < kNumPairClasses; ++c) {
+    const long long f = B.class_first[c], n = B.class_count[c];
+    for (long long i = 0; i < n; ++i) ks[f + i] = q[f + i];
+    std::sort(ks.begin() + f, ks.begin() + f + n, [](double x, double y) { return x > y; });
+  }
+  // pairs (i in bra class, j in ket class) with ks_i ks_j < t; for a triangular block the
+  // unordered pairs, diagonal included
+  auto below = [&](const HostBlock& h, double t) -> long long {
+    if (t <= 0.0) return 0;
+    const long long fb = B.class_first[h.cb], nb = B.class_count[h.cb];
+    const long long fk = B.class_first[h.ck], nk = B.class_count[h.ck];
+    long long ordered = 0, diag = 0;
+    for (long long i = 0; i < nb; ++i) {
+      const double v = ks[fb + i];
+      const long long ge = v > 0.0 ? count_ge(ks.data() + fk, nk, t / v) : 0;
+      ordered += nk - ge;
+      if (h.tri && !(v * v >= t)) ++diag;
+    }
+    return h.tri ? (ordered + diag) / 2 : ordered;
+  };
+  const int nblk = (int)B.blocks.size();
+  B.mix_n32.assign(nblk, 0);
+  B.mix_nskip.assign(nblk, 0);
+  for (int k = 0; k < nblk; ++k) {
+    const HostBlock& h = B.blocks[k];
+    B.mix_nskip[k] = below(h, skip * (1.0 + 1e-9));
+    B.mix_n32[k] = block_has_fp32(h) ? std::max<long long>(
+                                           0, below(h, fp32 * (1.0 + 1e-9)) - below(h, skip * (1.0 - 1e-9)))
+                                      : 0;
+  }
+  B.mix_key_skip = skip;
+  B.mix_key_fp32 = fp32;
+  return GBX_OK;
+}
+
 int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32) {
   int s;
   const bool mixed = skip > 0.0 || fp32 > 0.0;
@@ -829,15 +884,20 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
     return set_error(GBX_ERR_UNSUPPORTED, "the mixed-precision form computes 1/r integrals only");
   if (tau > 0.0 && (s = ensure_schwarz(B, st))) return s;
   if (mixed && (s = ensure_mixed_bounds(B, st))) return s;
+  if (mixed && (s = ensure_mixed_counts(B, skip, fp32))) return s;
   if ((s = ensure_full_work(B))) return s;
   if ((s = B.ensure_scratch(B.compact_elems, 0))) return s;
   const int nblk = (int)B.blocks.size();
   if (mixed && !B.d_counts32) {
     if ((s = B.alloc((void**)&B.d_counts32, nblk * sizeof(int), "cudaMalloc(counts32)"))) return s;
   }
+  B.counts_on_host = false;
   GBX_CUDA(cudaMemsetAsync(B.d_counts, 0, nblk * sizeof(int), st), "clear counts");
   if (mixed) GBX_CUDA(cudaMemsetAsync(B.d_counts32, 0, nblk * sizeof(int), st), "clear counts");
-  if (tau > 0.0 || skip > 0.0) {
+  long long left_out = 0;
+  if (mixed)
+    for (long long v : B.mix_nskip) left_out += v;
+  if (tau > 0.0 || left_out > 0) {
     // screened-out quartets are zero in the output: clear the store first
     GBX_CUDA(cudaMemsetAsync(B.d_compact, 0, B.compact_elems * sizeof(double), st),
              "clear compact store");
@@ -878,15 +938,21 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
     a.variant = h.variant;
     a.potential = B.potential;
     a.omega = B.omega;
+    // launch grids from the quartets each list can hold (FP64: all but those left out and
+    // the FP32 ones; the kernels read the exact counts from the device)
+    const long long n32 = mixed ? B.mix_n32[k] : 0;
+    const long long n64 = mixed ? std::max<long long>(1, h.ncand - B.mix_nskip[k] - n32 + 1) : h.ncand;
     const int grid = (int)std::max<long long>(
-        1, std::min<long long>((h.ncand * h.team + 127) / 128, (long long)nsm * h.ctas_per_sm));
+        1, std::min<long long>((n64 * h.team + 127) / 128, (long long)nsm * h.ctas_per_sm));
     if (per_block) cudaEventRecord(B.blk_ev[i], st);
     if ((s = launch_class(la, lb, lc, ld, a, grid, bs))) return s;
-    if (mixed && block_has_fp32(h)) {  // the block's FP32 list
+    if (n32 > 0) {  // the block's FP32 list
       a.work_count = B.d_counts32 + k;
       a.reverse = 1;
       a.fp32 = 1;
-      if ((s = launch_class(la, lb, lc, ld, a, grid, bs))) return s;
+      const int grid32 = (int)std::max<long long>(
+          1, std::min<long long>((n32 * h.team + 127) / 128, (long long)nsm * h.ctas_per_sm));
+      if ((s = launch_class(la, lb, lc, ld, a, grid32, bs))) return s;
     }
   }
   if (per_block) cudaEventRecord(B.blk_ev[nblk], st);
@@ -922,13 +988,6 @@ __global__ void expand_jwork(const long long* __restrict__ row_start, int nrows,
   }
   work[t] = make_int2(perm_b[lo], perm_k[first_col[lo] + (int)(w - row_start[lo])]);
 }
-
-namespace {
-// number of entries of the descending array k[0..n) that are >= x
-inline long long count_ge(const double* k, long long n, double x) {
-  return std::upper_bound(k, k + n, x, [](double v, double e) { return v > e; }) - k;
-}
-}  // namespace
 
 int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st, double skip,
                 double fp32) {
@@ -967,6 +1026,7 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
   std::vector<long long> rows;
   std::vector<int> cols;
   long long computed = 0, candidates = 0;
+  for (HostBlock& hb : B.blocks) hb.j_computed = 0;
   const double lo64 = mixed ? std::max(fp32, skip) : tau;  // FP64 when the bound is >= lo64
   const double lo = mixed ? skip : tau;                     // computed when the bound is >= lo
   for (int k = 0; k < (int)B.blocks.size(); ++k) {
@@ -997,11 +1057,13 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
       }
       L.total = rows.back();
       computed += L.total;
+      B.blocks[k].j_computed += L.total;
       if (L.total > 0) lists.push_back(L);
     }
   }
   B.last_computed = computed;
   B.last_screened = candidates - computed;
+  B.counts_on_host = true;
   GBX_CUDA(cudaMemsetAsync(J, 0, (size_t)B.nbf * B.nbf * sizeof(double), st), "clear J");
   if (lists.empty()) return GBX_OK;
   // device copies (one block, kept by the basis until the next call)
@@ -1034,22 +1096,8 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
       return s;
     B.jwork_cap = chunk * nstreams;
   }
-  GBX_CUDA(cudaEventRecord(B.fork, st), "fork");
-  for (int j = 0; j < nstreams; ++j) GBX_CUDA(cudaStreamWaitEvent(B.aux[j], B.fork, 0), "fork wait");
-  // largest lists first, round robin over the streams
-  std::vector<int> order(lists.size());
-  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    const HostBlock& hx = B.blocks[lists[x].blk];
-    const HostBlock& hy = B.blocks[lists[y].blk];
-    return lists[x].total * hx.avg_prims > lists[y].total * hy.avg_prims;
-  });
   const int nsm = num_sms(B.device);
-  for (size_t oi = 0; oi < order.size(); ++oi) {
-    const JList& L = lists[order[oi]];
-    const int j = (int)(oi % nstreams);
-    const cudaStream_t bs = B.aux[j];
-    int2* wk = B.d_jwork + (size_t)j * chunk;
+  auto launch_list = [&](const JList& L, cudaStream_t bs, int2* wk) -> int {
     const HostBlock& h = B.blocks[L.blk];
     for (long long w0 = 0; w0 < L.total; w0 += chunk) {
       const long long len = std::min(chunk, L.total - w0);
@@ -1073,10 +1121,39 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
       a.nbf = B.nbf;
       const int grid = (int)std::max<long long>(
           1, std::min<long long>((len * h.team + 127) / 128, (long long)nsm * h.ctas_per_sm));
-      if ((s = launch_class(kPairClassL[h.cb][0], kPairClassL[h.cb][1], kPairClassL[h.ck][0],
-                            kPairClassL[h.ck][1], a, grid, bs)))
-        return s;
+      int s2 = launch_class(kPairClassL[h.cb][0], kPairClassL[h.cb][1], kPairClassL[h.ck][0],
+                            kPairClassL[h.ck][1], a, grid, bs);
+      if (s2) return s2;
     }
+    return GBX_OK;
+  };
+  const int nblk = (int)B.blocks.size();
+  if (B.profiling && B.profile_level >= 2 && (int)B.blk_ev.size() == nblk + 1) {
+    // per-block timing: the blocks one after another on the caller's stream, in launch order
+    std::vector<std::vector<int>> of_block(nblk);
+    for (size_t li = 0; li < lists.size(); ++li) of_block[lists[li].blk].push_back((int)li);
+    for (int i = 0; i < nblk; ++i) {
+      const int k = B.launch_order.empty() ? i : B.launch_order[i];
+      cudaEventRecord(B.blk_ev[i], st);
+      for (int li : of_block[k])
+        if ((s = launch_list(lists[li], st, B.d_jwork))) return s;
+    }
+    cudaEventRecord(B.blk_ev[nblk], st);
+    return GBX_OK;
+  }
+  GBX_CUDA(cudaEventRecord(B.fork, st), "fork");
+  for (int j = 0; j < nstreams; ++j) GBX_CUDA(cudaStreamWaitEvent(B.aux[j], B.fork, 0), "fork wait");
+  // largest lists first, round robin over the streams
+  std::vector<int> order(lists.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    const HostBlock& hx = B.blocks[lists[x].blk];
+    const HostBlock& hy = B.blocks[lists[y].blk];
+    return lists[x].total * hx.avg_prims > lists[y].total * hy.avg_prims;
+  });
+  for (size_t oi = 0; oi < order.size(); ++oi) {
+    const int j = (int)(oi % nstreams);
+    if ((s = launch_list(lists[order[oi]], B.aux[j], B.d_jwork + (size_t)j * chunk))) return s;
   }
   for (int j = 0; j < nstreams; ++j) {
     GBX_CUDA(cudaEventRecord(B.join[j], B.aux[j]), "join");

@@ -652,7 +652,7 @@ int gbx_block_info(const gbx_basis* b, int k, int* cls4, int* team, double* avg_
   }
   if (team) *team = h.team;
   if (avg_prims) *avg_prims = h.avg_prims;
-  if (n_quartets) *n_quartets = h.ncand;
+  if (n_quartets) *n_quartets = B.counts_on_host ? h.j_computed : h.ncand;
   return GBX_OK;
 }
 
@@ -717,6 +717,11 @@ int gbx_basis_set_groups(gbx_basis* b, const int* group) {
 int gbx_last_counts(const gbx_basis* b, int64_t* computed, int64_t* screened) {
   if (!b) return set_error(GBX_ERR_INVALID, "gbx_last_counts: null basis");
   Basis& B = *b->impl;
+  if (B.counts_on_host) {
+    if (computed) *computed = B.last_computed;
+    if (screened) *screened = B.last_screened;
+    return GBX_OK;
+  }
   DeviceGuard g(B.device);
   const int nblk = (int)B.blocks.size();
   std::vector<int> c(nblk);

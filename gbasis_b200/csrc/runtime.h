@@ -29,6 +29,7 @@ struct HostBlock {
   int team = 1;            // lanes per quartet (register kernel), set by heuristic or autotuner
   int variant = 0;         // heavy classes with both kernels: 0 split, 1 line kernel
   int ctas_per_sm = 8;     // grid cap of the register kernel: resident-CTA multiples of the SMs
+  long long j_computed = 0;  // quartets the last direct-J call computed in this block
 };
 
 struct Basis {
@@ -88,6 +89,10 @@ struct Basis {
   bool mixed_ready = false;  // d_qmixed holds the final-value bounds
   std::vector<double> h_q;  // per pair, original-shell-pair bound
   long long last_computed = 0, last_screened = 0;
+  bool counts_on_host = false;
+  // mixed form: per block, upper bounds of the FP32 and left-out quartets at (skip, fp32)
+  std::vector<long long> mix_n32, mix_nskip;
+  double mix_key_skip = -1.0, mix_key_fp32 = -1.0;  // the last call counted its quartets on the host (direct J)
   // optional phase timing with events on the launching stream:
   // [0] work-list build, [1] class kernels, [2] expansion
   bool profiling = false;

@@ -234,8 +234,10 @@ int gbx_phase_times(gbx_basis* b, double* ms3);
 
 /* Work decomposition per class block (the autotuner's knobs): a class block is the set of
  * quartets of one (bra pair class, ket pair class); `team` is how many lanes share one
- * quartet's primitive loop in the register kernel (power of two, 1..32).  With profiling on,
- * gbx_block_times returns each block's kernel time of the last call (ms). */
+ * quartet's primitive loop in the register kernel (power of two, 1..32); n_quartets is the
+ * block's unique quartets (after a direct-J call: the quartets that call computed).  With
+ * profiling on, gbx_block_times returns each block's kernel time of the last call (ms); level 2
+ * also times the blocks of a direct-J call. */
 int gbx_num_blocks(const gbx_basis* b, int* n);
 int gbx_block_info(const gbx_basis* b, int k, int* cls4, int* team, double* avg_prims,
                    int64_t* n_quartets);

@@ -57,6 +57,7 @@ __all__ = [
     "generate_transformation",
     "quartet_cartesian",
     "construct_array_contraction",
+    "construct_array_contraction_by_primitive",
     "construct_array",
     "construct_array_lincomb",
     "electron_repulsion_integral",
@@ -397,6 +398,41 @@ def _exponent_oriented(sa, sb, sc, sd, potential=(0, 0.0)):
     inv = list(np.argsort(perm))
     x = np.transpose(x, inv + [4 + v for v in inv])
     return np.transpose(x, (4, 0, 5, 1, 6, 2, 7, 3))
+
+
+def construct_array_contraction_by_primitive(sa, sb, sc, sd):
+    """(M1, L1, M2, L2, M3, L3, M4, L4) as ``construct_array_contraction``, summed primitive
+    quartet by primitive quartet, each with its own recursion order: within each pair the
+    recursions run from the primitive of larger exponent (``_exponent_oriented`` on one-
+    primitive shells), and the horizontal recursion is applied per primitive quartet before
+    the sum.  Same mathematics as the contracted form (the contraction is linear); it is the
+    checker for heavily contracted shells whose primitives span tight and diffuse exponents,
+    where a contracted recursion run from one fixed centre per pair (the reference's form,
+    ``_two_elec_int.py:350-788``) loses up to about 1e-9 absolute: a primitive pair whose
+    other primitive is the tighter one puts the product centre P near the other atom, and the
+    vertical recursion then builds high angular momentum on a centre far from P."""
+    def one(shell, k):
+        cf = np.asarray(shell.coeffs, dtype=float).reshape(len(shell.exps), -1)
+        return _PrimShell(shell, k, cf[k])
+    out = 0.0
+    for i in range(len(sa.exps)):
+        for j in range(len(sb.exps)):
+            for k in range(len(sc.exps)):
+                for l in range(len(sd.exps)):
+                    out = out + _exponent_oriented(one(sa, i), one(sb, j), one(sc, k), one(sd, l))
+    return out
+
+
+class _PrimShell:
+    """Primitive k of a shell as a one-primitive shell (same centre, angular momentum,
+    component orders and coefficient row)."""
+
+    def __init__(self, shell, k, coef_row):
+        self.coord = shell.coord
+        self.angmom = shell.angmom
+        self.exps = np.asarray([float(np.asarray(shell.exps)[k])])
+        self.coeffs = np.asarray(coef_row, dtype=float).reshape(1, -1)
+        self.angmom_components_cart = shell.angmom_components_cart
 
 
 # --------------------------------------------------------------------- assembly

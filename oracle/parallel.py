@@ -89,7 +89,10 @@ def _blocks(quartets):
     sh, reorder, W = _W["shells"], _W["reorder"], _W["W"]
     out = []
     for i, j, k, l in quartets:
-        raw = orc.construct_array_contraction(sh[i], sh[j], sh[k], sh[l], reorder=reorder)
+        if reorder == "by_primitive":
+            raw = orc.construct_array_contraction_by_primitive(sh[i], sh[j], sh[k], sh[l])
+        else:
+            raw = orc.construct_array_contraction(sh[i], sh[j], sh[k], sh[l], reorder=reorder)
         s = raw.shape
         blk = raw.reshape(s[0] * s[1], s[2] * s[3], s[4] * s[5], s[6] * s[7])
         out.append(np.einsum("pa,qb,rc,sd,abcd->pqrs", W[i], W[j], W[k], W[l], blk).ravel())
@@ -119,7 +122,10 @@ def _chunks(quartets, n):
 
 def oracle_blocks(workload, quartets, processes=None, chunk=256, reorder="exponent"):
     """Flattened output-function blocks ([a][b][c][d] order) of ``quartets`` (rows of shell
-    indices of the workload ``workload``), concatenated in the given order."""
+    indices of the workload ``workload``), concatenated in the given order.  ``reorder``:
+    ``"exponent"`` (the engine's recursion order), ``False`` (the reference's own order) or
+    ``"by_primitive"`` (``construct_array_contraction_by_primitive``: each primitive quartet in
+    its own order, the accurate checker for heavily contracted shells)."""
     import multiprocessing as mp
     processes = processes or os.cpu_count() or 1
     with mp.get_context("spawn").Pool(processes, initializer=_init,

@@ -156,3 +156,21 @@ def test_horton_large_exponent_quartet():
     blk = orc.construct_array_contraction(shells[2], shells[3], shells[0], shells[1],
                                           reorder="exponent")
     assert abs(blk[0, i[2], 0, i[3], 0, i[0], 0, i[1]] - truth) <= ATOL
+
+
+def test_heavily_contracted_quartet_pins_the_primitive_wise_checker():
+    """A (dd|dd) quartet of the batch workload with d shells of 4-6 primitives spanning tight
+    and diffuse exponents (``heavy_contraction.npz``, written from gbasis itself and from
+    40-digit arithmetic).  The reference's own block misses the 40-digit values by about 5e-10,
+    and the oracle in the reference's order by the same order of magnitude (the two differ by
+    rounding, which this quartet amplifies a millionfold); the primitive-by-primitive form,
+    the checker of the GPU test on such quartets, matches the 40-digit values."""
+    from gbasis_b200.synthetic import batch_molecule
+    z = load_npz("heavy_contraction.npz")
+    shells = [batch_molecule(int(z["molecule"]))[int(i)] for i in z["quartet"]]
+    ref, truth = z["reference"], z["truth_40_digits"]
+    assert 1e-11 < float(np.abs(ref - truth).max()) < 1e-8
+    plain = orc.construct_array_contraction(*shells)
+    assert 1e-11 < float(np.abs(plain - truth).max()) < 1e-8
+    by_prim = orc.construct_array_contraction_by_primitive(*shells)
+    np.testing.assert_allclose(by_prim, truth, rtol=0, atol=1e-15)
