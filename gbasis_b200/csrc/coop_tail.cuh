@@ -256,7 +256,8 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
   const long long nBo = sB.nout, nDo = sD.nout;
   long long bbase, bcols;
   block_dest(a, P, bbase, bcols);
-  double* __restrict__ dst = a.out + bbase + Q.fo;
+  const bool tr = quartet_transposed(P, Q);  // values stored at [ket row][bra column]
+  double* __restrict__ dst = a.out + bbase;
   for (int c0 = 0; c0 < ncol; c0 += A.Cc) {
     const int cc = min(A.Cc, ncol - c0);
     for (int i = lane; i < cc * M.NE; i += 32) {
@@ -342,8 +343,9 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
       }
       const double v = OB[c * NAB + ua * nBi + ub] * sA.scl[ua] * sB.scl[ub] * sC.scl[uc] *
                        sD.scl[ud];
-      dst[((long long)P.fo + sA.pos[ua] * nBo + sB.pos[ub]) * bcols + sC.pos[uc] * nDo +
-          sD.pos[ud]] = v;
+      const long long rab = (long long)P.fo + sA.pos[ua] * nBo + sB.pos[ub];
+      const long long rcd = (long long)Q.fo + sC.pos[uc] * nDo + sD.pos[ud];
+      dst[tr ? rcd * bcols + rab : rab * bcols + rcd] = v;
     }
     __syncwarp();
   }

@@ -381,7 +381,11 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
     const long long nBo = sB.nout, nDo = sD.nout;
     long long bbase, bcols;
     block_dest(a, P, bbase, bcols);
-    double* __restrict__ dst = a.out + bbase + Q.fo;
+    // element (ab|cd) at [bra pair function][ket pair function], or transposed
+    // (quartet_transposed): strides of the bra and ket pair-function indices
+    const bool tr = quartet_transposed(P, Q);
+    const long long sbra = tr ? 1 : bcols, sket = tr ? bcols : 1;
+    double* __restrict__ dst = a.out + bbase;
 #pragma unroll
     for (int ia = 0; ia < NCA; ++ia) {
       if (ia >= nAi) break;
@@ -391,16 +395,17 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
       for (int ib = 0; ib < NCB; ++ib) {
         if (ib >= nBi) break;
         const double fab = fa * sB.scl[ib];
-        double* __restrict__ row = dst + (ra + sB.pos[ib]) * bcols;
+        double* __restrict__ row = dst + (ra + sB.pos[ib]) * sbra;
 #pragma unroll
         for (int ic = 0; ic < NCC; ++ic) {
           if (ic >= nCi) break;
           const double fabc = fab * sC.scl[ic];
-          double* __restrict__ rc = row + sC.pos[ic] * nDo;
+          const long long rc = (long long)Q.fo + sC.pos[ic] * nDo;
 #pragma unroll
           for (int id = 0; id < NCD; ++id) {
             if (id >= nDi) break;
-            rc[sD.pos[id]] = out[((ia * NCB + ib) * NCC + ic) * NCD + id] * fabc * sD.scl[id];
+            row[(rc + sD.pos[id]) * sket] =
+                out[((ia * NCB + ib) * NCC + ic) * NCD + id] * fabc * sD.scl[id];
           }
         }
       }

@@ -59,8 +59,23 @@ struct PairDev {
   int shA, shB, prim_off, nprim;
   int cls, local, fo, nB;  // class, index within class, pair-function offset in class, nout(B)
   double ABx, ABy, ABz;
-  int mol, pad;            // molecule of the pair in a batch (0 for a single basis)
+  int mol;                 // molecule of the pair in a batch (0 for a single basis)
+  // conditioning of the recursions run from this pair as the bra: the largest |P - A|
+  // sqrt(zeta) over its kept primitive pairs (0 for a one-centre pair); see pair_orient()
+  float orient;
 };
+
+// Primitive pairs whose product factor exp(-ab/zeta |AB|^2) is below e^{-69} (1e-30) are left
+// out of the primitive-pair lists (pair_precompute).
+constexpr double kPrimPairCut = 69.0;
+
+// A quartet of a diagonal class block (bra and ket pairs of one class) runs with either pair
+// as the bra: the one whose recursions are better conditioned (smaller `orient`).  Its values
+// belong to the block's entry whose row pair has the larger index in the class, so a quartet
+// run with the other pair as the bra stores them transposed.
+__device__ __forceinline__ bool quartet_transposed(const PairDev& P, const PairDev& Q) {
+  return P.cls == Q.cls && P.local < Q.local;
+}
 
 // Per class block: where its quartets live in the work list and in the compact store.
 struct BlockDev {

@@ -289,7 +289,10 @@ __device__ __forceinline__ void lines_tail(const EriLaunch& a, const double* ACC
   const int ncol = nCi * nDi;
   long long bbase, bcols;
   block_dest(a, P, bbase, bcols);
-  double* __restrict__ dst = a.out + bbase + Q.fo;
+  // strides of the bra and ket pair-function indices (transposed: quartet_transposed)
+  const bool tr = quartet_transposed(P, Q);
+  const long long sbra = tr ? 1 : bcols, sket = tr ? bcols : 1;
+  double* __restrict__ dst = a.out + bbase;
   const long long nBo = sB.nout, nDo = sD.nout;
   double mx = 0.0;
   for (int k = lane; k < ncol; k += 32) {
@@ -308,7 +311,7 @@ __device__ __forceinline__ void lines_tail(const EriLaunch& a, const double* ACC
     if (LB >= 2 && sB.sph) sph_axis<LB, NCA, 1>(o);
     if (LA >= 2 && sA.sph) sph_axis<LA, 1, NCB>(o);
     const double fcd = sC.scl[uc] * sD.scl[ud];
-    double* __restrict__ col = dst + sC.pos[uc] * nDo + sD.pos[ud];
+    double* __restrict__ col = dst + ((long long)Q.fo + sC.pos[uc] * nDo + sD.pos[ud]) * sket;
 #pragma unroll
     for (int ia = 0; ia < NCA; ++ia) {
       if (ia >= nAi) break;
@@ -317,7 +320,7 @@ __device__ __forceinline__ void lines_tail(const EriLaunch& a, const double* ACC
 #pragma unroll
       for (int ib = 0; ib < NCB; ++ib) {
         if (ib >= nBi) break;
-        col[(ra + sB.pos[ib]) * bcols] = o[ia * NCB + ib] * fa * sB.scl[ib];
+        col[(ra + sB.pos[ib]) * sbra] = o[ia * NCB + ib] * fa * sB.scl[ib];
       }
     }
   }
@@ -454,6 +457,7 @@ struct SplitQuartet {
   double pab[3], qab[3];
   int shA, shB, shC, shD;
   int pfo, qfo, mol, bra;
+  int tr, pad;  // stored transposed (quartet_transposed)
 };
 
 // Row stride of the split kernel's shared accumulators: a row holds NF values of [e0|f0] and,
@@ -524,7 +528,9 @@ __device__ __forceinline__ void split_tail(const EriLaunch& a, double* ACC,
     }
     const long long nBo = sB.nout, nDo = sD.nout;
     const double fcd = sC.scl[uc] * sD.scl[ud];
-    double* __restrict__ col = a.out + bbase + s.qfo + sC.pos[uc] * nDo + sD.pos[ud];
+    const long long sbra = s.tr ? 1 : bcols, sket = s.tr ? bcols : 1;
+    double* __restrict__ col =
+        a.out + bbase + ((long long)s.qfo + sC.pos[uc] * nDo + sD.pos[ud]) * sket;
 #pragma unroll
     for (int ia = 0; ia < NCA; ++ia) {
       if (ia >= nAi) break;
@@ -533,7 +539,7 @@ __device__ __forceinline__ void split_tail(const EriLaunch& a, double* ACC,
 #pragma unroll
       for (int ib = 0; ib < NCB; ++ib) {
         if (ib >= nBi) break;
-        col[(ra + sB.pos[ib]) * bcols] = o[ia * NCB + ib] * fa * sB.scl[ib];
+        col[(ra + sB.pos[ib]) * sbra] = o[ia * NCB + ib] * fa * sB.scl[ib];
       }
     }
   }
@@ -590,6 +596,7 @@ __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
         s.qfo = Q.fo;
         s.mol = P.mol;
         s.bra = pq.x;
+        s.tr = quartet_transposed(P, Q) ? 1 : 0;
       }
       double acc[C::kAcc];
 #pragma unroll

@@ -169,7 +169,8 @@ extern "C" int gbx_eri_full_noalloc(int n_shells, const int* angmom, const int* 
   build_work<<<(int)cmap.size(), 256, 0, st>>>(reinterpret_cast<const int2*>(base + o_cmap),
                                                reinterpret_cast<const BuildBlock*>(base + o_bb),
                                                nullptr, 0.0, d_work, d_counts,
-                                               MixedParams{nullptr, 0.0, 0.0, nullptr});
+                                               MixedParams{nullptr, 0.0, 0.0, nullptr},
+                                               d_pairs);
   if ((s = cuda_status(cudaGetLastError(), "build_work launch"))) return s;
   int nsm = 1;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);

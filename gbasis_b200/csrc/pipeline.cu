@@ -31,7 +31,15 @@ namespace gbx {
 // ------------------------------------------------------------------- K1
 // Reference: gbasis/integrals/_two_elec_int.py:306-322 (exponent sums, product centres,
 // relative coordinates) and :335-348, :528-547 (prefactor and primitive normalisation).
-__global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,
+//
+// Primitive pairs whose Gaussian-product factor exp(-ab/zeta |AB|^2) is below e^{-69}
+// (1e-30, kPrimPairCut) are left out: a normalised primitive pair's charge distribution is
+// bounded by that factor times powers of the distances that stay far below 1e10 here, so every
+// integral they would add is below 1e-20.  On a pair of tight primitives on different atoms the
+// factor is e^{-500} and less.  The kept ones are stored first, in their original order, and the
+// pair's primitive count on the device becomes theirs (at least one is kept).
+
+__global__ void pair_precompute(PairDev* __restrict__ pairs, int npairs,
                                 const ShellDev* __restrict__ shells,
                                 const double* __restrict__ exps, const double* __restrict__ coefs,
                                 PrimPair* __restrict__ prims) {
@@ -42,6 +50,14 @@ __global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,
   const ShellDev& B = shells[P.shB];
   const double ab2 = P.ABx * P.ABx + P.ABy * P.ABy + P.ABz * P.ABz;
   const double kpi = 5.914967172795613;  // sqrt(2) pi^{5/4}
+  // the smallest exponent argument of the pair: that primitive pair is always kept
+  double xmin = 1e300;
+  for (int ia = 0; ia < A.nprim; ++ia)
+    for (int ib = 0; ib < B.nprim; ++ib) {
+      const double a = exps[A.prim_off + ia], b = exps[B.prim_off + ib];
+      xmin = fmin(xmin, a * b / (a + b) * ab2);
+    }
+  int kept = 0;
   for (int ia = 0; ia < A.nprim; ++ia) {
     const double a = exps[A.prim_off + ia];
     const double na = coefs[A.prim_off + ia] * pow(2.0 * a / 3.14159265358979323846, 0.75) *
@@ -51,6 +67,8 @@ __global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,
       const double nb = coefs[B.prim_off + ib] * pow(2.0 * b / 3.14159265358979323846, 0.75) *
                         pow(4.0 * b, 0.5 * B.l);
       const double z = a + b, iz = 1.0 / z;
+      const double x = a * b * iz * ab2;
+      if (x > kPrimPairCut && x > xmin) continue;
       PrimPair r;
       r.zeta = z;
       r.izeta = iz;
@@ -60,11 +78,12 @@ __global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,
       r.Xx = r.Px - A.x;
       r.Xy = r.Py - A.y;
       r.Xz = r.Pz - A.z;
-      r.C = kpi * na * nb * exp(-a * b * iz * ab2) * iz;
+      r.C = kpi * na * nb * exp(-x) * iz;
       r.pad = 0.0;
-      prims[P.prim_off + ia * B.nprim + ib] = r;
+      prims[P.prim_off + kept++] = r;
     }
   }
+  pairs[p].nprim = kept;
 }
 
 // ------------------------------------------------------------------- K2
@@ -101,7 +120,8 @@ __global__ void build_work_range(const BuildBlock B, long long start, long long 
 
 __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* __restrict__ bb,
                            const double* __restrict__ qs, double tau, int2* __restrict__ work,
-                           int* __restrict__ counts, const MixedParams mp) {
+                           int* __restrict__ counts, const MixedParams mp,
+                           const PairDev* __restrict__ pairs) {
   const int2 cm = cta_map[blockIdx.x];
   const BuildBlock B = bb[cm.x];
   const long long t = (long long)cm.y + threadIdx.x;
@@ -126,8 +146,14 @@ __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* _
       // of each shell) decides skip (< skip), FP32 (< fp32) or FP64
       const double bnd = mp.qm[p] * mp.qm[q];
       if (bnd < mp.skip) pass = false;
-      fp32 = pass && B.fp32_ok && bnd < mp.fp32;
+      fp32 = pass && B.fp32_ok && (!mp.fp32_on || mp.fp32_on[B.blk]) && bnd < mp.fp32;
     }
+  }
+  // diagonal blocks: the better-conditioned pair is the bra (quartet_transposed)
+  if (B.tri && pairs && pass && pairs[q].orient < pairs[p].orient) {
+    const int t2 = p;
+    p = q;
+    q = t2;
   }
   const bool p64 = pass && !fp32;
   const unsigned mask = __ballot_sync(0xffffffffu, p64);
@@ -865,13 +891,22 @@ static int ensure_mixed_counts(Basis& B, double skip, double fp32) {
   const int nblk = (int)B.blocks.size();
   B.mix_n32.assign(nblk, 0);
   B.mix_nskip.assign(nblk, 0);
+  std::vector<int> on(nblk, 0);
   for (int k = 0; k < nblk; ++k) {
     const HostBlock& h = B.blocks[k];
     B.mix_nskip[k] = below(h, skip * (1.0 + 1e-9));
     B.mix_n32[k] = block_has_fp32(h) ? std::max<long long>(
                                            0, below(h, fp32 * (1.0 + 1e-9)) - below(h, skip * (1.0 - 1e-9)))
                                       : 0;
+    // an FP32 list pays for its own launch only when it holds a share of the block; the
+    // quartets of a smaller one stay in the FP64 list
+    on[k] = B.mix_n32[k] >= kMinFp32List && B.mix_n32[k] * 20 >= h.ncand;
+    if (!on[k]) B.mix_n32[k] = 0;
   }
+  if (!B.d_fp32_on && B.alloc((void**)&B.d_fp32_on, nblk * sizeof(int), "cudaMalloc(fp32 flags)"))
+    return GBX_ERR_OOM;
+  GBX_CUDA(cudaMemcpy(B.d_fp32_on, on.data(), nblk * sizeof(int), cudaMemcpyHostToDevice),
+           "upload fp32 flags");
   B.mix_key_skip = skip;
   B.mix_key_fp32 = fp32;
   return GBX_OK;
@@ -902,10 +937,12 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
     GBX_CUDA(cudaMemsetAsync(B.d_compact, 0, B.compact_elems * sizeof(double), st),
              "clear compact store");
   }
-  const MixedParams mp{B.d_qmixed, skip, fp32, mixed ? B.d_counts32 : nullptr};
+  const MixedParams mp{B.d_qmixed, skip, fp32, mixed ? B.d_counts32 : nullptr,
+                       mixed ? B.d_fp32_on : nullptr};
   if (B.profiling) cudaEventRecord(B.ev[0], st);
   build_work<<<B.n_cta_build, 256, 0, st>>>(B.d_cta_map, (const BuildBlock*)B.d_build_blocks,
-                                            B.d_qscreen, tau, B.d_work, B.d_counts, mp);
+                                            B.d_qscreen, tau, B.d_work, B.d_counts, mp,
+                                            B.d_pairs);
   GBX_CUDA(cudaGetLastError(), "build_work launch");
   if (B.profiling) cudaEventRecord(B.ev[1], st);
   const int nsm = num_sms(B.device);
@@ -976,7 +1013,7 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
 __global__ void expand_jwork(const long long* __restrict__ row_start, int nrows,
                              const int* __restrict__ first_col, const int* __restrict__ perm_b,
                              const int* __restrict__ perm_k, long long w0, long long len,
-                             int2* __restrict__ work) {
+                             int2* __restrict__ work, const PairDev* __restrict__ pairs, int tri) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= len) return;
   const long long w = w0 + t;
@@ -986,7 +1023,13 @@ __global__ void expand_jwork(const long long* __restrict__ row_start, int nrows,
     if (row_start[mid] <= w) lo = mid;
     else hi = mid - 1;
   }
-  work[t] = make_int2(perm_b[lo], perm_k[first_col[lo] + (int)(w - row_start[lo])]);
+  int p = perm_b[lo], q = perm_k[first_col[lo] + (int)(w - row_start[lo])];
+  if (tri && pairs[q].orient < pairs[p].orient) {  // the better-conditioned pair as the bra
+    const int t2 = p;
+    p = q;
+    q = t2;
+  }
+  work[t] = make_int2(p, q);
 }
 
 int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st, double skip,
@@ -1103,7 +1146,7 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
       const long long len = std::min(chunk, L.total - w0);
       expand_jwork<<<(int)((len + 255) / 256), 256, 0, bs>>>(
           d_rows + L.row_off, L.nrows, d_cols + L.col_off, d_perm + B.class_first[h.cb],
-          d_perm + B.class_first[h.ck], w0, len, wk);
+          d_perm + B.class_first[h.ck], w0, len, wk, B.d_pairs, h.tri ? 1 : 0);
       GBX_CUDA(cudaGetLastError(), "expand_jwork launch");
       EriLaunch a = base_launch(B);
       a.work = wk;

@@ -32,7 +32,7 @@ struct ExpandArgs {
   long long pf_first[kNumPairClasses + 1];
 };
 
-__global__ void pair_precompute(const PairDev* __restrict__ pairs, int npairs,
+__global__ void pair_precompute(PairDev* __restrict__ pairs, int npairs,
                                 const ShellDev* __restrict__ shells,
                                 const double* __restrict__ exps, const double* __restrict__ coefs,
                                 PrimPair* __restrict__ prims);
@@ -41,11 +41,13 @@ struct MixedParams {
   const double* qm;  // per pair: Schwarz bound x largest output scale of its two shells
   double skip, fp32;
   int* counts32;
+  const int* fp32_on;  // per block: 1 = FP32 list in use (nullptr: every block with an FP32 path)
 };
 
 __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* __restrict__ bb,
                            const double* __restrict__ qs, double tau, int2* __restrict__ work,
-                           int* __restrict__ counts, const MixedParams mp);
+                           int* __restrict__ counts, const MixedParams mp,
+                           const PairDev* __restrict__ pairs);
 __global__ void expand_full(const ExpandArgs e);
 __global__ void expand_rows(const ExpandArgs e);
 __global__ void build_work_range(const BuildBlock B, long long start, long long len,

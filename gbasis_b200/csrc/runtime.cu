@@ -87,6 +87,33 @@ int boys_table(int device, const double** out) {
 }
 
 // ------------------------------------------------------------------ basis setup
+// Conditioning of a pair's recursions when it is the bra: the vertical recursion builds
+// angular momentum on A from the product centre P of each primitive pair, and its values grow
+// like (|P - A| sqrt(zeta))^e while the results the horizontal recursion makes of them do not;
+// a diffuse A primitive with a tight B primitive puts P near B.  The score is the largest
+// |P - A| sqrt(zeta) = b |AB| / sqrt(a + b) over the primitive pairs pair_precompute keeps.
+// Measured on 151 same-class (dd|dd) quartets of the batch workload against values summed
+// primitive quartet by primitive quartet: the bra in the reference's order missed by up to
+// 8.3e-7; the pair of smaller score as the bra by at most 2.6e-9, the best either order gives.
+float pair_orient(const ShellDev& A, const ShellDev& Bs, const double* exps, double ab2) {
+  const double ab = sqrt(ab2);
+  double xmin = 1e300;
+  for (int i = 0; i < A.nprim; ++i)
+    for (int j = 0; j < Bs.nprim; ++j) {
+      const double a = exps[A.prim_off + i], b = exps[Bs.prim_off + j];
+      xmin = std::min(xmin, a * b / (a + b) * ab2);
+    }
+  double sc = 0.0;
+  for (int i = 0; i < A.nprim; ++i)
+    for (int j = 0; j < Bs.nprim; ++j) {
+      const double a = exps[A.prim_off + i], b = exps[Bs.prim_off + j];
+      const double x = a * b / (a + b) * ab2;
+      if (x > kPrimPairCut && x > xmin) continue;
+      sc = std::max(sc, b * ab / sqrt(a + b));
+    }
+  return (float)sc;
+}
+
 struct DeviceGuard {
   int prev = -1;
   explicit DeviceGuard(int dev) {
@@ -319,6 +346,7 @@ int build_basis(Basis& B, int n, const int* angmom, const int* nprim, const doub
     d.ABx = B.shells[h.a].x - B.shells[h.b].x;
     d.ABy = B.shells[h.a].y - B.shells[h.b].y;
     d.ABz = B.shells[h.a].z - B.shells[h.b].z;
+    d.orient = pair_orient(B.shells[h.a], B.shells[h.b], exps, d.ABx * d.ABx + d.ABy * d.ABy + d.ABz * d.ABz);
     prim_pairs += h.nprim;
     // orientation bit: 1 if the first function index of the ordered pair (i,j) lives
     // on the pair's B shell

@@ -13,6 +13,7 @@ namespace gbx {
 
 constexpr int kAuxStreams = 6;      // default concurrent class-block streams of a basis
 constexpr int kMaxAuxStreams = 16;  // the most a basis may be given
+constexpr long long kMinFp32List = 2048;  // mixed form: smallest FP32 list given its own launch
 constexpr long long kCoulombChunk = 1LL << 23;  // quartets per direct-Coulomb work chunk
 constexpr int kStageBuffers = 3;                // host-output staging slabs in flight
 constexpr size_t kStageBytes = 64ull << 20;     // target bytes of one staging slab
@@ -92,7 +93,8 @@ struct Basis {
   bool counts_on_host = false;
   // mixed form: per block, upper bounds of the FP32 and left-out quartets at (skip, fp32)
   std::vector<long long> mix_n32, mix_nskip;
-  double mix_key_skip = -1.0, mix_key_fp32 = -1.0;  // the last call counted its quartets on the host (direct J)
+  double mix_key_skip = -1.0, mix_key_fp32 = -1.0;
+  int* d_fp32_on = nullptr;  // per block: FP32 list in use  // the last call counted its quartets on the host (direct J)
   // optional phase timing with events on the launching stream:
   // [0] work-list build, [1] class kernels, [2] expansion
   bool profiling = false;
