@@ -112,6 +112,7 @@ __device__ __forceinline__ int n_int(const ShellDev& s) {
 // and m upward steps F_{k+1} = ((2k+1) F_k - e^{-T})/(2T).
 __device__ __forceinline__ double boys_lane_value(int m, double T, const double* __restrict__ tab) {
   double f;
+  T = fmax(T, 0.0);  // T >= 0 by construction; the table is never indexed below its start
   if (T < kBoysTMax) {
     const int n = __double2int_rn(T * 10.0);
     const double x = fma(-T, 10.0, (double)n) * 0.1;

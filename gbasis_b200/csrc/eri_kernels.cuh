@@ -28,6 +28,7 @@ __device__ __forceinline__ constexpr double inv_odd(int m) { return 1.0 / (2 * m
 template <int L>
 __device__ __forceinline__ void boys_eval(double T, const double* __restrict__ s_tab,
                                           const double* __restrict__ s_exp, double* F) {
+  T = fmax(T, 0.0);  // T >= 0 by construction; the table is never indexed below its start
   if (T < kBoysTMax) {
     const int n = __double2int_rn(T * 10.0);
     const double x = fma(-T, 10.0, (double)n) * 0.1;  // T_n - T
@@ -68,6 +69,7 @@ template <int L>
 __device__ __forceinline__ void boys_accumulate(double T, const double* __restrict__ s_tab,
                                                 const double* __restrict__ s_exp, double c0,
                                                 double sc, double* F) {
+  T = fmax(T, 0.0);
   if (T < kBoysTMax) {
     const int n = __double2int_rn(T * 10.0);
     const double x = fma(-T, 10.0, (double)n) * 0.1;

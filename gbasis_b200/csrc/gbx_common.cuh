@@ -66,8 +66,29 @@ struct PairDev {
 };
 
 // Primitive pairs whose product factor exp(-ab/zeta |AB|^2) is below e^{-69} (1e-30) are left
-// out of the primitive-pair lists (pair_precompute).
+// out of the primitive-pair lists (pair_precompute), except the pair's one of smallest argument.
 constexpr double kPrimPairCut = 69.0;
+
+// ab/(a+b) |AB|^2: the one expression for the product factor's argument, host and device.
+__host__ __device__ inline double prim_pair_arg(double a, double b, double ab2) {
+  return a * b / (a + b) * ab2;
+}
+
+// Index ia * nb + ib of the primitive pair of smallest argument (the first one on ties).
+__host__ __device__ inline int kept_primitive_pair(const double* ea, int na, const double* eb,
+                                                   int nb, double ab2) {
+  double xmin = 0.0;
+  int best = 0;
+  for (int i = 0; i < na; ++i)
+    for (int j = 0; j < nb; ++j) {
+      const double x = prim_pair_arg(ea[i], eb[j], ab2);
+      if ((i == 0 && j == 0) || x < xmin) {
+        xmin = x;
+        best = i * nb + j;
+      }
+    }
+  return best;
+}
 
 // A quartet of a diagonal class block (bra and ket pairs of one class) runs with either pair
 // as the bra: the one whose recursions are better conditioned (smaller `orient`).  Its values

@@ -405,6 +405,10 @@ __global__ void __launch_bounds__(128, 4) eri_lines(const CoopArgs A) {
       bp = bpn;
       kp = kpn;
     }
+    if (np == 0) {  // no primitive quartet (a pair left without primitives): zero targets
+      for (int i = lane; i < C::NE * C::NF; i += 32) ACC[i] = 0.0;
+      __syncwarp();
+    }
     if constexpr (C::kRegTail && !COULOMB) {
       lines_tail<C::LA, C::LB, C::LC, C::LD, typename C::Tail>(a, S, S + C::NE * C::NF, pq, P, Q,
                                                                lane, C::NE, C::NF);

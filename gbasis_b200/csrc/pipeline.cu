@@ -50,13 +50,9 @@ __global__ void pair_precompute(PairDev* __restrict__ pairs, int npairs,
   const ShellDev& B = shells[P.shB];
   const double ab2 = P.ABx * P.ABx + P.ABy * P.ABy + P.ABz * P.ABz;
   const double kpi = 5.914967172795613;  // sqrt(2) pi^{5/4}
-  // the smallest exponent argument of the pair: that primitive pair is always kept
-  double xmin = 1e300;
-  for (int ia = 0; ia < A.nprim; ++ia)
-    for (int ib = 0; ib < B.nprim; ++ib) {
-      const double a = exps[A.prim_off + ia], b = exps[B.prim_off + ib];
-      xmin = fmin(xmin, a * b / (a + b) * ab2);
-    }
+  // the primitive pair of smallest exponent argument is always kept (found with the same
+  // expression as below, so the pair's list is never empty)
+  const int keep0 = kept_primitive_pair(exps + A.prim_off, A.nprim, exps + B.prim_off, B.nprim, ab2);
   int kept = 0;
   for (int ia = 0; ia < A.nprim; ++ia) {
     const double a = exps[A.prim_off + ia];
@@ -67,8 +63,8 @@ __global__ void pair_precompute(PairDev* __restrict__ pairs, int npairs,
       const double nb = coefs[B.prim_off + ib] * pow(2.0 * b / 3.14159265358979323846, 0.75) *
                         pow(4.0 * b, 0.5 * B.l);
       const double z = a + b, iz = 1.0 / z;
-      const double x = a * b * iz * ab2;
-      if (x > kPrimPairCut && x > xmin) continue;
+      const double x = prim_pair_arg(a, b, ab2);
+      if (x > kPrimPairCut && ia * B.nprim + ib != keep0) continue;
       PrimPair r;
       r.zeta = z;
       r.izeta = iz;
@@ -775,7 +771,10 @@ static int ensure_mixed_bounds(Basis& B, cudaStream_t st) {
   const int np = (int)B.pairs.size();
   if (!B.d_qmixed && (s = B.alloc((void**)&B.d_qmixed, np * sizeof(double), "cudaMalloc(qmixed)")))
     return s;
-  std::vector<PairDev> tp(B.pairs);
+  // the device's pair records: their primitive counts are those pair_precompute kept
+  std::vector<PairDev> tp(np);
+  GBX_CUDA(cudaMemcpy(tp.data(), B.d_pairs, np * sizeof(PairDev), cudaMemcpyDeviceToHost),
+           "download pairs");
   std::vector<int2> diag(np);
   std::vector<long long> off(np + 1, 0), ncols(np);
   for (int p = 0; p < np; ++p) {

@@ -97,18 +97,12 @@ int boys_table(int device, const double** out) {
 // 8.3e-7; the pair of smaller score as the bra by at most 2.6e-9, the best either order gives.
 float pair_orient(const ShellDev& A, const ShellDev& Bs, const double* exps, double ab2) {
   const double ab = sqrt(ab2);
-  double xmin = 1e300;
-  for (int i = 0; i < A.nprim; ++i)
-    for (int j = 0; j < Bs.nprim; ++j) {
-      const double a = exps[A.prim_off + i], b = exps[Bs.prim_off + j];
-      xmin = std::min(xmin, a * b / (a + b) * ab2);
-    }
+  const int keep0 = kept_primitive_pair(exps + A.prim_off, A.nprim, exps + Bs.prim_off, Bs.nprim, ab2);
   double sc = 0.0;
   for (int i = 0; i < A.nprim; ++i)
     for (int j = 0; j < Bs.nprim; ++j) {
       const double a = exps[A.prim_off + i], b = exps[Bs.prim_off + j];
-      const double x = a * b / (a + b) * ab2;
-      if (x > kPrimPairCut && x > xmin) continue;
+      if (prim_pair_arg(a, b, ab2) > kPrimPairCut && i * Bs.nprim + j != keep0) continue;
       sc = std::max(sc, b * ab / sqrt(a + b));
     }
   return (float)sc;
