@@ -291,9 +291,8 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
 
     const int nprim = valid ? P.nprim * Q.nprim : 0;
     int ip = tl / Q.nprim, jq = tl - ip * Q.nprim;
-    // one primitive quartet (bra primitive pair ipx, ket jqx) with weight w into accr
-    auto prim_quartet = [&](int ipx, int jqx, double w) {
-      const PrimPair bp = a.prims[P.prim_off + ipx];
+    // one primitive quartet (bra primitive pair bp, ket jqx) with weight w into accr
+    auto prim_quartet = [&](const PrimPair& bp, int jqx, double w) {
       const double o2z = 0.5 * bp.izeta;
       const PrimPair kp = a.prims[Q.prim_off + jqx];
       const double r = rsqrt(bp.zeta + kp.zeta);
@@ -332,8 +331,15 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
         ++ip;
       }
     };
+    // the bra primitive pair changes every Q.nprim / team steps: loaded only then
+    PrimPair bp;
+    int bp_ip = -1;
     for (int idx = tl; idx < nprim; idx += team) {
-      prim_quartet(ip, jq, 1.0);
+      if (ip != bp_ip) {
+        bp = a.prims[P.prim_off + ip];
+        bp_ip = ip;
+      }
+      prim_quartet(bp, jq, 1.0);
       advance();
     }
     double acc[C::NE * C::NF];

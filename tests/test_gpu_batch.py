@@ -119,9 +119,8 @@ def _stretched(mol, f):
 
 
 def test_batch_mixed_form_against_fp64_and_single_path():
-    """Mixed form of the batch: within 1e-10 of the FP64 batch, equal (1e-12) to the
-    single-basis mixed form of each molecule, graph replay reproducible, and the FP64 graph
-    unaffected.  Two molecules are stretched (x4, x3) so that the batch has quartets left out
+    """Mixed form of the batch: within 1e-10 of the FP64 batch, as the single-basis mixed form
+    of each molecule is, graph replay reproducible, and the FP64 graph unaffected.  Two molecules are stretched (x4, x3) so that the batch has quartets left out
     (bounds far below 1e-11) and FP32 quartets (light-class bounds in [1e-9, 2e-8]).  The
     thresholds are fixed here (skip 1e-11, FP32 2e-7: more FP32 quartets than the default);
     on this batch they keep the error within 1e-10."""
@@ -156,7 +155,11 @@ def test_batch_mixed_form_against_fp64_and_single_path():
                        stream=ctypes.c_void_p(torch.cuda.current_stream().cuda_stream), mixed=th)
         torch.cuda.synchronize()
         db.close()
-        np.testing.assert_allclose(got.reshape(-1), single.cpu().numpy(), rtol=0, atol=1e-12)
+        # the single-basis form keeps a block's FP32 quartets in FP64 when they are too few
+        # for their own launch, the batch runs them in FP32: both within the mixed bar
+        single = single.cpu().numpy()
+        assert np.max(np.abs(single - ref.reshape(-1))) <= 1e-10, m
+        np.testing.assert_allclose(got.reshape(-1), single, rtol=0, atol=2e-10)
     b.close()
     outs = electron_repulsion_integral_batch(mols[:2], notation="chemist", precision="mixed",
                                              mixed_skip=th[0], mixed_fp32=th[1])
