@@ -10,6 +10,7 @@
 // contraction, HRR, component norm) and gbasis/base_four_symm.py:195-349 (norm_cont,
 // spherical transform).
 #pragma once
+#include <type_traits>
 #include "gbx_common.cuh"
 #include "eri_gen.cuh"
 
@@ -291,8 +292,9 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
 
     const int nprim = valid ? P.nprim * Q.nprim : 0;
     int ip = tl / Q.nprim, jq = tl - ip * Q.nprim;
-    // one primitive quartet (bra primitive pair bp, ket jqx) with weight w into accr
-    auto prim_quartet = [&](const PrimPair& bp, int jqx, double w) {
+    // one primitive quartet (bra primitive pair ipx, ket jqx) into accr
+    auto prim_quartet = [&](int ipx, int jqx) {
+      const PrimPair bp = a.prims[P.prim_off + ipx];
       const double o2z = 0.5 * bp.izeta;
       const PrimPair kp = a.prims[Q.prim_off + jqx];
       const double r = rsqrt(bp.zeta + kp.zeta);
@@ -304,7 +306,7 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
       boys_eval<L>(T, s_tab, s_exp, F);
       if constexpr (ATT)
         boys_attenuate<L>(a.potential, a.omega, bp.zeta * rz, T, s_tab, s_exp, F);
-      const double pref = bp.C * kp.C * r * w;
+      const double pref = bp.C * kp.C * r;
 #pragma unroll
       for (int m = 0; m <= L; ++m) F[m] *= pref;
       const double ze = bp.zeta * kp.izeta;
@@ -331,15 +333,8 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
         ++ip;
       }
     };
-    // the bra primitive pair changes every Q.nprim / team steps: loaded only then
-    PrimPair bp;
-    int bp_ip = -1;
     for (int idx = tl; idx < nprim; idx += team) {
-      if (ip != bp_ip) {
-        bp = a.prims[P.prim_off + ip];
-        bp_ip = ip;
-      }
-      prim_quartet(bp, jq, 1.0);
+      prim_quartet(ip, jq);
       advance();
     }
     double acc[C::NE * C::NF];
@@ -390,34 +385,38 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
     long long bbase, bcols;
     block_dest(a, P, bbase, bcols);
     // element (ab|cd) at [bra pair function][ket pair function], or transposed
-    // (quartet_transposed): strides of the bra and ket pair-function indices
-    const bool tr = quartet_transposed(P, Q);
-    const long long sbra = tr ? 1 : bcols, sket = tr ? bcols : 1;
-    double* __restrict__ dst = a.out + bbase;
+    // (quartet_transposed: a diagonal-block quartet run from its lower pair)
+    auto store = [&](auto transposed) {
+      constexpr bool TR = decltype(transposed)::value;
+      double* __restrict__ dst = a.out + bbase;
 #pragma unroll
-    for (int ia = 0; ia < NCA; ++ia) {
-      if (ia >= nAi) break;
-      const double fa = sA.scl[ia];
-      const long long ra = (long long)P.fo + sA.pos[ia] * nBo;
+      for (int ia = 0; ia < NCA; ++ia) {
+        if (ia >= nAi) break;
+        const double fa = sA.scl[ia];
+        const long long ra = (long long)P.fo + sA.pos[ia] * nBo;
 #pragma unroll
-      for (int ib = 0; ib < NCB; ++ib) {
-        if (ib >= nBi) break;
-        const double fab = fa * sB.scl[ib];
-        double* __restrict__ row = dst + (ra + sB.pos[ib]) * sbra;
+        for (int ib = 0; ib < NCB; ++ib) {
+          if (ib >= nBi) break;
+          const double fab = fa * sB.scl[ib];
+          const long long rab = ra + sB.pos[ib];
 #pragma unroll
-        for (int ic = 0; ic < NCC; ++ic) {
-          if (ic >= nCi) break;
-          const double fabc = fab * sC.scl[ic];
-          const long long rc = (long long)Q.fo + sC.pos[ic] * nDo;
+          for (int ic = 0; ic < NCC; ++ic) {
+            if (ic >= nCi) break;
+            const double fabc = fab * sC.scl[ic];
+            const long long rc = (long long)Q.fo + sC.pos[ic] * nDo;
 #pragma unroll
-          for (int id = 0; id < NCD; ++id) {
-            if (id >= nDi) break;
-            row[(rc + sD.pos[id]) * sket] =
-                out[((ia * NCB + ib) * NCC + ic) * NCD + id] * fabc * sD.scl[id];
+            for (int id = 0; id < NCD; ++id) {
+              if (id >= nDi) break;
+              const long long rcd = rc + sD.pos[id];
+              dst[TR ? rcd * bcols + rab : rab * bcols + rcd] =
+                  out[((ia * NCB + ib) * NCC + ic) * NCD + id] * fabc * sD.scl[id];
+            }
           }
         }
       }
-    }
+    };
+    if (quartet_transposed(P, Q)) store(std::true_type{});
+    else store(std::false_type{});
   }
 }
 
