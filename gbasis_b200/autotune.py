@@ -181,3 +181,33 @@ def autotune(shells, coord_types=None, reps=3, teams=TEAMS, ctas=CTAS, streams=S
             json.dump(table, f, indent=1, sort_keys=True)
     db.close()
     return chosen, timings
+
+
+def main(argv):
+    """``python -m gbasis_b200.autotune medium8 chain20 batch512``: tune the named synthetic
+    workloads in order (the stream count of the last single-basis workload wins; the batch keeps
+    the single-basis stream count) and store the choices in the cache."""
+    import torch
+    from .synthetic import make_workload
+    for name in argv:
+        if name == "batch512":
+            from .batch import EriBatch
+            b = EriBatch(make_workload("batch512"))
+            outs = [torch.empty((n,) * 4, dtype=torch.float64, device="cuda") for n in b.nbf]
+            chosen, _ = b.autotune(outs)
+            b.close()
+        else:
+            keep = _load().get("streams")
+            chosen, _ = autotune(make_workload(name))
+            if keep is not None and name != argv[0]:
+                # the first single-basis workload sets the stream count
+                table = _load()
+                table["streams"] = keep
+                with open(cache_path(), "w") as f:
+                    json.dump(table, f, indent=1, sort_keys=True)
+        print(name, json.dumps(chosen, sort_keys=True), flush=True)
+
+
+if __name__ == "__main__":
+    import sys
+    main(sys.argv[1:])

@@ -356,7 +356,7 @@ def emit_sources(outdir, heavy, nfiles=12):
             launchers[c] = name
             out.append(f"int {name}(const EriLaunch& a, cudaStream_t st) {{")
             if split_ok(c):
-                out.append(f"  if (a.mode != 2 && a.variant == 0) return launch_split_t<SplitCls_{tag}>(a, st);")
+                out.append(f"  if (a.variant == 0) return launch_split_t<SplitCls_{tag}>(a, st);")
             out.append(f"  return launch_lines_t<LinesCls_{tag}>(a, kCoopMeta[{j}], st);")
             out.append("}")
         out.append("}  // namespace gbx")

@@ -461,7 +461,7 @@ struct SplitQuartet {
   double pab[3], qab[3];
   int shA, shB, shC, shD;
   int pfo, qfo, mol, bra;
-  int tr, pad;  // stored transposed (quartet_transposed)
+  int tr, ket;  // stored transposed (quartet_transposed); ket pair (Coulomb mode)
 };
 
 // Row stride of the split kernel's shared accumulators: a row holds NF values of [e0|f0] and,
@@ -476,11 +476,15 @@ __host__ __device__ constexpr int split_rs(int nf, int ncd) { return (nf > ncd ?
 template <int LA, int LB, int LC, int LD, class T, int NE, int RS>
 __device__ __forceinline__ void split_tail(const EriLaunch& a, double* ACC,
                                            const SplitQuartet* sq, unsigned long long* s_mx,
-                                           int nq) {
+                                           int nq, double* JAB) {
   constexpr int NCA = ncart(LA), NCB = ncart(LB), NCC = ncart(LC), NCDD = ncart(LD);
   constexpr int NCD = NCC * NCDD, NAB = NCA * NCB;
   constexpr int QS = NE * RS;
   const bool schwarz = a.mode == 1;
+  const bool coulomb = a.mode == 2;  // J: JAB[q][ab] gathers sum_cd (ab|cd) D[c][d] per quartet
+  if (coulomb) {
+    for (int i = threadIdx.x; i < nq * NAB; i += blockDim.x) JAB[i] = 0.0;
+  }
   for (int t = threadIdx.x; t < nq * NE; t += blockDim.x) {
     const int q = t / NE, e = t - q * NE;
     const SplitQuartet& s = sq[q];
@@ -522,6 +526,33 @@ __device__ __forceinline__ void split_tail(const EriLaunch& a, double* ACC,
     }
     if (LB >= 2 && sB.sph) sph_axis<LB, NCA, 1>(o);
     if (LA >= 2 && sA.sph) sph_axis<LA, 1, NCB>(o);
+    if (coulomb) {
+      // J[a][b] += (1 + [C != D]) sum_cd (ab|cd) D[c][d] (gathered in JAB, added below) and,
+      // for a quartet whose pairs differ, J[c][d] += (1 + [A != B]) sum_ab (ab|cd) D[a][b]
+      const long long n = a.nbf;
+      const long long fc = sC.func_off + sC.pos[uc], fd = sD.func_off + sD.pos[ud];
+      const double fcd = sC.scl[uc] * sD.scl[ud];
+      const double dcd = a.D[fc * n + fd] * fcd;
+      double scd = 0.0;
+#pragma unroll
+      for (int ia = 0; ia < NCA; ++ia) {
+        if (ia >= nAi) break;
+#pragma unroll
+        for (int ib = 0; ib < NCB; ++ib) {
+          if (ib >= nBi) break;
+          const double v = o[ia * NCB + ib];
+          atomicAdd(JAB + q * NAB + ia * NCB + ib, v * dcd);
+          scd = fma(v, a.D[(sA.func_off + sA.pos[ia]) * n + sB.func_off + sB.pos[ib]] *
+                           (sA.scl[ia] * sB.scl[ib]), scd);
+        }
+      }
+      if (s.bra != s.ket) {
+        const double w = scd * ((s.shA != s.shB) ? 2.0 : 1.0) * fcd;
+        atomicAdd(a.J + fc * n + fd, w);
+        if (s.shC != s.shD) atomicAdd(a.J + fd * n + fc, w);
+      }
+      continue;
+    }
     long long bbase, bcols;
     if (a.mol_base) {
       bbase = a.mol_base[s.mol];
@@ -552,14 +583,29 @@ __device__ __forceinline__ void split_tail(const EriLaunch& a, double* ACC,
     for (int q = threadIdx.x; q < nq; q += blockDim.x)
       a.qout[sq[q].bra] = sqrt(__longlong_as_double((long long)s_mx[q]));
   }
+  if (coulomb) {
+    __syncthreads();
+    const long long n = a.nbf;
+    for (int t = threadIdx.x; t < nq * NAB; t += blockDim.x) {
+      const int q = t / NAB, i = t - q * NAB, ia = i / NCB, ib = i - ia * NCB;
+      const SplitQuartet& s = sq[q];
+      const ShellDev& sA = a.shells[s.shA];
+      const ShellDev& sB = a.shells[s.shB];
+      if (ia >= internal_count(sA) || ib >= internal_count(sB)) continue;
+      const long long fa = sA.func_off + sA.pos[ia], fb = sB.func_off + sB.pos[ib];
+      const double v = JAB[t] * ((s.shC != s.shD) ? 2.0 : 1.0) * sA.scl[ia] * sB.scl[ib];
+      atomicAdd(a.J + fa * n + fb, v);
+      if (s.shA != s.shB) atomicAdd(a.J + fb * n + fa, v);
+    }
+  }
 }
 
 // Split register kernel for heavy classes of moderate size: a CTA of S = C::kS warps (4 or 8)
 // takes 32 quartets at a time, thread t of warp r computing part r (a contiguous range of bra
 // rows e) of quartet t's contracted [e0|f0] in registers (generated straight-line recursions,
 // as in the light classes' kernel); the parts meet in shared memory ACC[32][NE][RS] and all
-// threads of the CTA then share the group's tail (split_tail).  Store (mode 0) and Schwarz
-// (mode 1) only.
+// threads of the CTA then share the group's tail (split_tail): store (mode 0), Schwarz
+// maximum (mode 1) or Coulomb-matrix contributions (mode 2).
 template <class C, bool ATT = false>
 __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
   __shared__ double s_tab[kBoysNGrid * kBoysTaylor];
@@ -601,6 +647,7 @@ __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
         s.mol = P.mol;
         s.bra = pq.x;
         s.tr = quartet_transposed(P, Q) ? 1 : 0;
+        s.ket = pq.y;
       }
       double acc[C::kAcc];
 #pragma unroll
@@ -636,7 +683,8 @@ __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
     }
     __syncthreads();
     const int nq = (int)(count - base < 32 ? count - base : 32);
-    split_tail<C::LA, C::LB, C::LC, C::LD, typename C::Tail, C::NE, RS>(a, ACC, sq, s_mx, nq);
+    split_tail<C::LA, C::LB, C::LC, C::LD, typename C::Tail, C::NE, RS>(a, ACC, sq, s_mx, nq,
+                                                                        ACC + 32 * QS);
     __syncthreads();
   }
 }
@@ -644,7 +692,10 @@ __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
 template <class C>
 int launch_split_t(const EriLaunch& a, cudaStream_t st) {
   constexpr int NCD = ncart(C::LC) * ncart(C::LD);
-  const size_t dyn = (size_t)32 * C::NE * split_rs(C::NF, NCD) * sizeof(double);
+  constexpr int NAB = ncart(C::LA) * ncart(C::LB);
+  // ACC[32][NE][RS]; the Coulomb mode adds the per-quartet sums JAB[32][NAB]
+  const size_t dyn = (size_t)32 * C::NE * split_rs(C::NF, NCD) * sizeof(double) +
+                     (a.mode == 2 ? (size_t)32 * NAB * sizeof(double) : 0);
   auto kern = a.potential ? eri_split<C, true> : eri_split<C>;
   int s = cuda_status(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)dyn), "eri_split shared memory attribute");
