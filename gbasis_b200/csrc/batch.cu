@@ -207,7 +207,8 @@ static int build_batch(Batch& Bt, int n_mol, const int* mol_nshells, const int* 
           for (long long ql = 0; ql < qn; ++ql) {
             const int q = (int)(pair_off[m] + fk + ql);
             // diagonal block types: the better-conditioned pair is the bra
-            if (cb == ck && pairs[q].orient < pairs[p].orient) work.push_back(make_int2(q, p));
+            if (block_orients(cb, ck) && pairs[q].orient < pairs[p].orient)
+              work.push_back(make_int2(q, p));
             else work.push_back(make_int2(p, q));
             prim_sum += (double)pairs[p].nprim * pairs[q].nprim;
           }

@@ -90,8 +90,9 @@ __host__ __device__ inline int kept_primitive_pair(const double* ea, int na, con
   return best;
 }
 
-// A quartet of a diagonal class block (bra and ket pairs of one class) runs with either pair
-// as the bra: the one whose recursions are better conditioned (smaller `orient`).  Its values
+// A quartet of a diagonal class block (bra and ket pairs of one class, lA + lB >= 3:
+// block_orients) runs with either pair as the bra: the one whose recursions are better
+// conditioned (smaller `orient`).  Its values
 // belong to the block's entry whose row pair has the larger index in the class, so a quartet
 // run with the other pair as the bra stores them transposed.
 __device__ __forceinline__ bool quartet_transposed(const PairDev& P, const PairDev& Q) {

@@ -99,7 +99,8 @@ extern "C" int gbx_eri_full_noalloc(int n_shells, const int* angmom, const int* 
   for (int k = 0; k < nblk; ++k) {
     const HostBlock& h = B.blocks[k];
     bb[k] = BuildBlock{(int)B.class_first[h.cb], (int)h.nb, (int)B.class_first[h.ck], (int)h.nk,
-                       h.tri ? 1 : 0, k, h.dev.work_off, h.ncand};
+                       h.tri ? 1 : 0, k, h.dev.work_off, h.ncand, 0,
+                       block_orients(h.cb, h.ck) ? 1 : 0};
     for (long long c0 = 0; c0 < h.ncand; c0 += 256) cmap.push_back(make_int2(k, (int)c0));
   }
   std::vector<int4> pinfo(np);

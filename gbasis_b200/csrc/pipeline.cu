@@ -146,7 +146,7 @@ __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* _
     }
   }
   // diagonal blocks: the better-conditioned pair is the bra (quartet_transposed)
-  if (B.tri && pairs && pass && pairs[q].orient < pairs[p].orient) {
+  if (B.orient && pairs && pass && pairs[q].orient < pairs[p].orient) {
     const int t2 = p;
     p = q;
     q = t2;
@@ -620,7 +620,8 @@ static int ensure_full_work(Basis& B) {
   for (int k = 0; k < nblk; ++k) {
     const HostBlock& h = B.blocks[k];
     bb[k] = BuildBlock{(int)B.class_first[h.cb], (int)h.nb, (int)B.class_first[h.ck], (int)h.nk,
-                       h.tri ? 1 : 0, k, h.dev.work_off, h.ncand, block_has_fp32(h) ? 1 : 0, 0};
+                       h.tri ? 1 : 0, k, h.dev.work_off, h.ncand, block_has_fp32(h) ? 1 : 0,
+                       block_orients(h.cb, h.ck) ? 1 : 0};
     for (long long c0 = 0; c0 < h.ncand; c0 += 256) cmap.push_back(make_int2(k, (int)c0));
     if (h.ncand > (1LL << 31) - 256)
       return set_error(GBX_ERR_UNSUPPORTED, "class block with %lld quartets exceeds the limit",
@@ -1145,7 +1146,8 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
       const long long len = std::min(chunk, L.total - w0);
       expand_jwork<<<(int)((len + 255) / 256), 256, 0, bs>>>(
           d_rows + L.row_off, L.nrows, d_cols + L.col_off, d_perm + B.class_first[h.cb],
-          d_perm + B.class_first[h.ck], w0, len, wk, B.d_pairs, h.tri ? 1 : 0);
+          d_perm + B.class_first[h.ck], w0, len, wk, B.d_pairs,
+          block_orients(h.cb, h.ck) ? 1 : 0);
       GBX_CUDA(cudaGetLastError(), "expand_jwork launch");
       EriLaunch a = base_launch(B);
       a.work = wk;

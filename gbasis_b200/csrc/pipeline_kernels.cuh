@@ -10,7 +10,7 @@ struct BuildBlock {
   int tri, blk;
   long long work_off, ncand;
   int fp32_ok;  // the block's class kernel has an FP32 path (mixed form); 0: FP64 only
-  int pad;
+  int orient;   // diagonal block whose quartets run from the better-conditioned pair
 };
 
 // Full-tensor expansion (K6).

@@ -21,6 +21,13 @@ constexpr size_t kStageBytes = 64ull << 20;     // target bytes of one staging s
 int boys_table(int device, const double** out);
 int compiled_lmax();
 
+// Diagonal blocks whose quartets run from the better-conditioned pair (quartet_transposed):
+// those of pairs with lA + lB >= 3, where a contracted recursion run from a poorly placed
+// centre loses digits; the lighter ones keep one orientation (no divergent stores).
+inline bool block_orients(int cb, int ck) {
+  return cb == ck && kPairClassL[cb][0] + kPairClassL[cb][1] >= 3;
+}
+
 struct HostBlock {
   int cb, ck;
   long long nb, nk, ncand;
