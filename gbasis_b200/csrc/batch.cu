@@ -54,6 +54,7 @@ struct Batch {
   double* d_coefs = nullptr;
   const double* d_boys = nullptr;
   int2* d_work = nullptr;
+  unsigned long long* d_tickets = nullptr;  // per type: its FP64 and FP32 lists' work counters
   double* d_compact = nullptr;
   int* d_gtab = nullptr;
   int4* d_rowinfo = nullptr;
@@ -301,6 +302,9 @@ static int build_batch(Batch& Bt, int n_mol, const int* mol_nshells, const int* 
   }
   if ((s = Bt.alloc((void**)&Bt.d_exp, n_mol * sizeof(ExpandArgs), "cudaMalloc(batch descriptors)")))
     return s;
+  if ((s = Bt.alloc((void**)&Bt.d_tickets, 2 * Bt.types.size() * sizeof(unsigned long long),
+                    "cudaMalloc(batch work counters)")))
+    return s;
   GBX_CUDA(cudaStreamCreateWithFlags(&Bt.exec, cudaStreamNonBlocking), "create stream");
   Bt.aux.resize(kAuxStreams);
   Bt.join.resize(kAuxStreams);
@@ -465,6 +469,10 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st, bool mixed = false) {
   if (mixed && Bt.mix_count[2] > 0)
     GBX_CUDA(cudaMemsetAsync(Bt.d_compact, 0, (size_t)Bt.compact_elems * sizeof(double), st),
              "clear batch compact store");
+  const bool tickets = !static_work_order();
+  if (tickets)
+    GBX_CUDA(cudaMemsetAsync(Bt.d_tickets, 0, 2 * Bt.types.size() * sizeof(unsigned long long), st),
+             "clear batch work counters");
   GBX_CUDA(cudaEventRecord(Bt.fork, st), "fork");
   for (cudaStream_t a : Bt.aux) GBX_CUDA(cudaStreamWaitEvent(a, Bt.fork, 0), "fork wait");
   for (size_t i = 0; i < Bt.order.size(); ++i) {
@@ -486,6 +494,7 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st, bool mixed = false) {
     a.variant = T.variant;
     a.mol_base = T.d_base;
     a.mol_ncols = T.d_ncols;
+    a.ticket = tickets ? Bt.d_tickets + 2 * k : nullptr;
     cudaStream_t ts = Bt.profile ? st : Bt.aux[i % Bt.aux.size()];
     if (mixed) {
       a.work = Bt.d_work_mixed;
@@ -503,6 +512,7 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st, bool mixed = false) {
       a.work_off = Bt.mix_off[k] + Bt.mix_n64[k];
       a.nwork = Bt.mix_n32[k];
       a.fp32 = 1;
+      a.ticket = tickets ? Bt.d_tickets + 2 * k + 1 : nullptr;
       const int grid = (int)std::max<long long>(
           1, std::min<long long>((a.nwork * T.team + 127) / 128, (long long)nsm * T.ctas_per_sm));
       int s = launch_class(kPairClassL[T.cb][0], kPairClassL[T.cb][1], kPairClassL[T.ck][0],

@@ -52,7 +52,9 @@ __global__ void eri_coop(const CoopArgs A) {
 
   const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + wib; w < count; w += nwarps) {
+  unsigned long long* const tk = a.ticket;  // one quartet per draw
+  for (long long w = tk ? warp_ticket(tk, lane) : (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+       w < count; w = tk ? warp_ticket(tk, lane) : w + nwarps) {
     const int2 pq = a.work[a.reverse ? a.work_off + a.nwork - 1 - w : a.work_off + w];
     const PairDev P = a.pairs[pq.x];
     const PairDev Q = a.pairs[pq.y];

@@ -279,6 +279,8 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
   __syncthreads();
   const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  // static order (a.ticket is not used: a step here is short, and one draw per warp and step
+  // from a shared counter measured 4 % slower on the 120-function full tensor)
   for (long long wb = gwarp * per_warp; wb < count; wb += nwarps * per_warp) {
     const long long w = wb + lane / team;
     const bool valid = w < count;

@@ -136,7 +136,20 @@ struct EriLaunch {
   double omega;
   // heavy classes that have both kernels: 0 = split register kernel, 1 = line kernel
   int variant;
+  // work counter of this launch, zero before it starts: in the heavy-class kernels warps (split
+  // kernel: CTAs) take their next quartets from it with atomicAdd, so that a CTA that becomes
+  // resident late (class blocks share the GPU with other blocks on other streams) takes less
+  // work.  nullptr, and in the light-class register kernel: the static order, quartet w to
+  // warp w mod (warps in the grid).
+  unsigned long long* ticket;
 };
+
+// Next work ticket of a warp (every lane of the warp calls it; lane 0 draws).
+__device__ __forceinline__ long long warp_ticket(unsigned long long* t, int lane) {
+  unsigned long long v = 0;
+  if (lane == 0) v = atomicAdd(t, 1ull);
+  return (long long)__shfl_sync(0xffffffffu, v, 0);
+}
 
 // Destination block of a quartet whose bra pair is P.
 __device__ __forceinline__ void block_dest(const EriLaunch& a, const PairDev& P, long long& base,

@@ -432,7 +432,11 @@ def emit_tail(cls):
 # ------------------------------------------------------------------- split register kernel
 SPLITS = (4, 8)     # warps of a CTA, each computing one part of the targets
 SPLIT_MAX_ACC = 64  # accumulators per thread in a part
-SPLIT_MAX_OPS = 500
+SPLIT_MAX_OPS = 500  # recursion operations per part with 4 parts
+# with 8 parts: every class of 620 < ops <= 750 (and every one of 500 < ops <= 620 with more
+# than 40 accumulators) was checked spill-free with ptxas on sm_100a (226-252 registers);
+# 906 ops spilled 220-530 bytes
+SPLIT_MAX_OPS_8 = 750
 SPLIT_MAX_L = 7
 
 
@@ -447,8 +451,8 @@ def split_parts(cls, S):
 def split_ok(cls):
     """Number of parts (warps) of the split kernel for the class, or 0: the smallest S whose
     parts fit a thread's registers (at most SPLIT_MAX_ACC accumulators and SPLIT_MAX_OPS
-    recursion operations per part, or 620 operations with at most 40 accumulators; beyond that
-    the parts spill, as measured with ptxas on sm_100a)."""
+    recursion operations per part, or 620 operations with at most 40 accumulators, or with 8
+    parts SPLIT_MAX_OPS_8; beyond that the parts spill, as measured with ptxas on sm_100a)."""
     return _split_ok(tuple(cls))
 
 
@@ -468,7 +472,7 @@ def _split_ok(cls):
         if acc > SPLIT_MAX_ACC:
             continue
         ops = max(_part_gen(cls, E[e0:e1], F).op_count() for e0, e1 in parts)
-        if ops <= SPLIT_MAX_OPS or (acc <= 40 and ops <= 620):
+        if ops <= SPLIT_MAX_OPS or (acc <= 40 and ops <= 620) or (S == 8 and ops <= SPLIT_MAX_OPS_8):
             return S
     return 0
 

@@ -364,7 +364,9 @@ __global__ void __launch_bounds__(128, 4) eri_lines(const CoopArgs A) {
   double* Fs = Y + C::kY;
   const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
   const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + wib; w < count; w += nwarps) {
+  unsigned long long* const tk = a.ticket;  // one quartet per draw
+  for (long long w = tk ? warp_ticket(tk, lane) : (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+       w < count; w = tk ? warp_ticket(tk, lane) : w + nwarps) {
     const int2 pq = a.work[a.reverse ? a.work_off + a.nwork - 1 - w : a.work_off + w];
     const PairDev P = a.pairs[pq.x];
     const PairDev Q = a.pairs[pq.y];
@@ -622,9 +624,17 @@ __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
   stage_boys<L>(a.boys_tab, s_tab, s_exp);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* ACC = dyn;
-  for (long long base = (long long)blockIdx.x * 32; base < count; base += (long long)gridDim.x * 32) {
+  // groups of 32 quartets: from the launch's work counter (thread 0 draws, the CTA reads it
+  // after the barrier; the next draw comes after the group's barriers), else every gridDim-th
+  __shared__ long long s_base;
+  unsigned long long* const tk = a.ticket;
+  long long base = (long long)blockIdx.x * 32;
+  for (;;) {
     if (threadIdx.x < 32) s_mx[threadIdx.x] = 0ull;
+    if (tk && threadIdx.x == 0) s_base = (long long)atomicAdd(tk, 1ull) * 32;
     __syncthreads();  // Boys table staged (first group); previous group's tail done
+    if (tk) base = s_base;
+    if (base >= count) break;  // the same for all threads of the CTA
     const long long w = base + lane;
     if (w < count) {
       const int2 pq = a.work[a.reverse ? a.work_off + a.nwork - 1 - w : a.work_off + w];
@@ -686,6 +696,7 @@ __global__ void __launch_bounds__(C::kS * 32) eri_split(const EriLaunch a) {
     split_tail<C::LA, C::LB, C::LC, C::LD, typename C::Tail, C::NE, RS>(a, ACC, sq, s_mx, nq,
                                                                         ACC + 32 * QS);
     __syncthreads();
+    base += (long long)gridDim.x * 32;  // static order (replaced by the next draw with a counter)
   }
 }
 

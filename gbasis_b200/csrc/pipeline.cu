@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -640,6 +641,34 @@ static int ensure_full_work(Basis& B) {
   return GBX_OK;
 }
 
+bool static_work_order() {
+  static const bool v = [] {
+    const char* e = std::getenv("GBX_WORK_ORDER");
+    return e && std::strcmp(e, "static") == 0;
+  }();
+  return v;
+}
+
+// n work counters for one call's class launches, zeroed on stream st; *t = nullptr when the
+// static order is chosen.
+static int ensure_tickets(Basis& B, long long n, cudaStream_t st, unsigned long long** t) {
+  *t = nullptr;
+  if (static_work_order() || n <= 0) return GBX_OK;
+  if (B.tickets_cap < n) {
+    if (B.d_tickets) B.release(B.d_tickets);
+    B.d_tickets = nullptr;
+    B.tickets_cap = 0;
+    int s = B.alloc((void**)&B.d_tickets, (size_t)n * sizeof(unsigned long long),
+                    "cudaMalloc(work counters)");
+    if (s) return s;
+    B.tickets_cap = n;
+  }
+  GBX_CUDA(cudaMemsetAsync(B.d_tickets, 0, (size_t)n * sizeof(unsigned long long), st),
+           "clear work counters");
+  *t = B.d_tickets;
+  return GBX_OK;
+}
+
 static EriLaunch base_launch(Basis& B) {
   EriLaunch a;
   memset(&a, 0, sizeof(a));
@@ -951,6 +980,8 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
   // order on the caller's stream instead.
   const bool per_block = B.profiling && B.profile_level >= 2;
   const int nstreams = per_block ? 0 : B.n_streams;
+  unsigned long long* tickets = nullptr;  // [2 k]: block k's FP64 list, [2 k + 1]: its FP32 list
+  if ((s = ensure_tickets(B, 2LL * nblk, st, &tickets))) return s;
   if (nstreams) {
     if ((s = ensure_aux_streams(B))) return s;
     GBX_CUDA(cudaEventRecord(B.fork, st), "fork");
@@ -975,6 +1006,7 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
     a.variant = h.variant;
     a.potential = B.potential;
     a.omega = B.omega;
+    a.ticket = tickets ? tickets + 2 * k : nullptr;
     // launch grids from the quartets each list can hold (FP64: all but those left out and
     // the FP32 ones; the kernels read the exact counts from the device)
     const long long n32 = mixed ? B.mix_n32[k] : 0;
@@ -987,6 +1019,7 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
       a.work_count = B.d_counts32 + k;
       a.reverse = 1;
       a.fp32 = 1;
+      a.ticket = tickets ? tickets + 2 * k + 1 : nullptr;
       const int grid32 = (int)std::max<long long>(
           1, std::min<long long>((n32 * h.team + 127) / 128, (long long)nsm * h.ctas_per_sm));
       if ((s = launch_class(la, lb, lc, ld, a, grid32, bs))) return s;
@@ -1140,7 +1173,14 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
     B.jwork_cap = chunk * nstreams;
   }
   const int nsm = num_sms(B.device);
-  auto launch_list = [&](const JList& L, cudaStream_t bs, int2* wk) -> int {
+  // one work counter per chunk launch, in list order
+  std::vector<long long> first_ticket(lists.size() + 1, 0);
+  for (size_t li = 0; li < lists.size(); ++li)
+    first_ticket[li + 1] = first_ticket[li] + (lists[li].total + chunk - 1) / chunk;
+  unsigned long long* tickets = nullptr;
+  if ((s = ensure_tickets(B, first_ticket.back(), st, &tickets))) return s;
+  auto launch_list = [&](int li, cudaStream_t bs, int2* wk) -> int {
+    const JList& L = lists[li];
     const HostBlock& h = B.blocks[L.blk];
     for (long long w0 = 0; w0 < L.total; w0 += chunk) {
       const long long len = std::min(chunk, L.total - w0);
@@ -1163,6 +1203,7 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
       a.D = D;
       a.J = J;
       a.nbf = B.nbf;
+      a.ticket = tickets ? tickets + first_ticket[li] + w0 / chunk : nullptr;
       const int grid = (int)std::max<long long>(
           1, std::min<long long>((len * h.team + 127) / 128, (long long)nsm * h.ctas_per_sm));
       int s2 = launch_class(kPairClassL[h.cb][0], kPairClassL[h.cb][1], kPairClassL[h.ck][0],
@@ -1180,7 +1221,7 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
       const int k = B.launch_order.empty() ? i : B.launch_order[i];
       cudaEventRecord(B.blk_ev[i], st);
       for (int li : of_block[k])
-        if ((s = launch_list(lists[li], st, B.d_jwork))) return s;
+        if ((s = launch_list(li, st, B.d_jwork))) return s;
     }
     cudaEventRecord(B.blk_ev[nblk], st);
     return GBX_OK;
@@ -1197,7 +1238,7 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
   });
   for (size_t oi = 0; oi < order.size(); ++oi) {
     const int j = (int)(oi % nstreams);
-    if ((s = launch_list(lists[order[oi]], B.aux[j], B.d_jwork + (size_t)j * chunk))) return s;
+    if ((s = launch_list(order[oi], B.aux[j], B.d_jwork + (size_t)j * chunk))) return s;
   }
   for (int j = 0; j < nstreams; ++j) {
     GBX_CUDA(cudaEventRecord(B.join[j], B.aux[j]), "join");

@@ -63,6 +63,8 @@ struct Basis {
   long long jwork_cap = 0;
   void* d_jplan = nullptr;   // direct Coulomb: row starts, pair order, first ket positions
   size_t jplan_bytes = 0;
+  unsigned long long* d_tickets = nullptr;  // work counters of one call's class launches
+  long long tickets_cap = 0;
   int* d_counts32 = nullptr;   // mixed form: FP32 quartets per block
   double* d_qmixed = nullptr;  // mixed form: per-pair bound of the final values
   std::vector<long long> class_first, class_count, class_funcs;
@@ -158,5 +160,8 @@ int launch_diagonal_bounds(const PairDev* pairs, int npairs, const ShellDev* she
                            const BlockDev* blocks, const double* compact, double* q,
                            cudaStream_t st);
 int launch_class(int la, int lb, int lc, int ld, const EriLaunch& a, int grid, cudaStream_t st);
+// GBX_WORK_ORDER=static: class kernels take their quartets in the static grid-stride order
+// instead of from per-launch work counters (read once per process; a diagnostic)
+bool static_work_order();
 
 }  // namespace gbx
