@@ -16,7 +16,12 @@ from .contractions import is_shell
 __all__ = ["lib", "EngineError", "check", "pack_basis", "DeviceBasis", "EXPORTED_SYMBOLS",
            "library_path", "fp64_peak", "release_cached_memory"]
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libgbx_eri.so")
+LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib")
+# GBX_DEBUG_BOUNDS=1 selects the bounds-checking build (python -m gbasis_b200.build
+# --debug-bounds): every store of the kernels is index-checked and a call that went out of
+# range returns an error instead of writing there
+LIB_PATH = os.path.join(LIB_DIR, "libgbx_eri_debug.so" if os.environ.get("GBX_DEBUG_BOUNDS") == "1"
+                        else "libgbx_eri.so")
 
 GBX_OK, GBX_ERR_INVALID, GBX_ERR_UNSUPPORTED, GBX_ERR_OOM, GBX_ERR_CUDA, GBX_ERR_TIMEOUT = range(6)
 GBX_CHEMIST, GBX_PHYSICIST = 0, 1
@@ -35,7 +40,8 @@ EXPORTED_SYMBOLS = (
     "gbx_batch_type_times", "gbx_release_cached_memory", "gbx_eri_jk", "gbx_point_charge",
     "gbx_basis_set_potential", "gbx_batch_run_mixed", "gbx_batch_mixed_counts", "gbx_boys_eval",
     "gbx_pipe_peak", "gbx_eri_coulomb_j_mixed", "gbx_set_block_config", "gbx_basis_set_streams",
-    "gbx_batch_set_type_config",
+    "gbx_batch_set_type_config", "gbx_mixed_counts", "gbx_batch_set_queue", "gbx_debug_bounds",
+    "gbx_basis_set_fp32_lists",
 )
 
 
@@ -78,6 +84,8 @@ def lib():
             "gbx_lincomb": [_P, _I64, _P, _I64, _P, _P, _P],
             "gbx_eri_coulomb_j": [_P, _P, _D, _P, _P],
             "gbx_last_counts": [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
+            "gbx_mixed_counts": [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64),
+                                 ctypes.POINTER(_I64)],
             "gbx_last_error": [ctypes.c_char_p, ctypes.c_size_t],
             "gbx_fp64_peak": [_I, ctypes.POINTER(_D)],
             "gbx_boys_eval": [_I, _I64, _P, _P],
@@ -102,6 +110,9 @@ def lib():
             "gbx_batch_info": [_P, _P, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
             "gbx_batch_run": [_P, _I, _P, _P],
             "gbx_batch_set_graph": [_P, _I],
+            "gbx_batch_set_queue": [_P, _I],
+            "gbx_debug_bounds": [ctypes.POINTER(_I)],
+            "gbx_basis_set_fp32_lists": [_P, _I64, _I64],
             "gbx_unique_values": [_P, _I64, _P, _P, _P],
             "gbx_compact_view": [_P, ctypes.POINTER(_P), ctypes.POINTER(_I64)],
             "gbx_batch_num_types": [_P, ctypes.POINTER(_I)],
@@ -383,6 +394,19 @@ class DeviceBasis:
         a, b = ctypes.c_int64(), ctypes.c_int64()
         check(lib().gbx_last_counts(self.handle, ctypes.byref(a), ctypes.byref(b)))
         return int(a.value), int(b.value)
+
+    def set_fp32_lists(self, min_quartets=65536, share=4):
+        """Mixed form: the smallest FP32 list (quartets, and share of its block) that gets
+        its own FP32 launch; smaller ones stay in the FP64 list."""
+        check(lib().gbx_basis_set_fp32_lists(self.handle, int(min_quartets), int(share)),
+              "gbx_basis_set_fp32_lists")
+
+    def mixed_counts(self):
+        """(FP64, FP32, left out) quartets of the last full-tensor or unique-integral call."""
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        check(lib().gbx_mixed_counts(self.handle, ctypes.byref(a), ctypes.byref(b),
+                                     ctypes.byref(c)), "gbx_mixed_counts")
+        return int(a.value), int(b.value), int(c.value)
 
     def set_potential(self, potential=0, omega=0.0):
         """Operator of later integral calls: 0 = 1/r, 1 = erf(omega r)/r, 2 = erfc(omega r)/r."""

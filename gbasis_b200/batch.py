@@ -66,6 +66,13 @@ class EriBatch:
         _engine.check(_engine.lib().gbx_batch_set_team(self.handle, int(k), int(team)),
                       "gbx_batch_set_team")
 
+    def set_queue(self, on=True):
+        """True: FP64 runs evaluate every block type in ONE persistent launch that drains a
+        single multi-class work queue (``gbx_batch_set_queue``); False: one class kernel per
+        block type (the default)."""
+        _engine.check(_engine.lib().gbx_batch_set_queue(self.handle, 1 if on else 0),
+                      "gbx_batch_set_queue")
+
     def apply_tuning(self, table=None):
         """Teams from the tuning cache (keyed by class and primitive bucket, shared with the
         single-basis tuner); returns how many types changed."""

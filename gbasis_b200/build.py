@@ -21,6 +21,9 @@ GEN = os.path.join(CSRC, "_gen")
 BUILD = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libgbx_eri.so")
+# bounds-checking build (GBX_DEBUG_BOUNDS=1): its own objects and library
+BUILD_DEBUG = os.path.join(HERE, "_build_debug")
+LIB_DEBUG = os.path.join(LIBDIR, "libgbx_eri_debug.so")
 LMAX_DEFAULT = 3
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -66,12 +69,12 @@ def _deps_mtime(src):
     return m
 
 
-def compile_one(src, force, verbose_ptxas=False):
-    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+def compile_one(src, force, verbose_ptxas=False, debug=False):
+    obj = os.path.join(BUILD_DEBUG if debug else BUILD, os.path.basename(src) + ".o")
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(
             os.path.getmtime(src), _deps_mtime(src)):
         return obj, 0.0, ""
-    cmd = [nvcc(), *NVCC_FLAGS, "-c", src, "-o", obj]
+    cmd = [nvcc(), *NVCC_FLAGS, *(["-DGBX_DEBUG_BOUNDS=1"] if debug else []), "-c", src, "-o", obj]
     if verbose_ptxas:
         cmd += ["-Xptxas", "-v"]
     t = time.time()
@@ -81,25 +84,28 @@ def compile_one(src, force, verbose_ptxas=False):
     return obj, time.time() - t, r.stderr
 
 
-def build(lmax=LMAX_DEFAULT, jobs=None, force=False, verbose=False, ptxas=False):
-    os.makedirs(BUILD, exist_ok=True)
+def build(lmax=LMAX_DEFAULT, jobs=None, force=False, verbose=False, ptxas=False, debug=False):
+    """Build the library; ``debug``: the bounds-checking one (libgbx_eri_debug.so)."""
+    lib_path = LIB_DEBUG if debug else LIB
+    os.makedirs(BUILD_DEBUG if debug else BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     srcs = sources(lmax)
     jobs = jobs or max(1, min(len(srcs), os.cpu_count() or 4))
     objs = []
     with cf.ThreadPoolExecutor(jobs) as ex:
-        for obj, dt, err in ex.map(lambda s: compile_one(s, force, ptxas), srcs):
+        for obj, dt, err in ex.map(lambda s: compile_one(s, force, ptxas, debug), srcs):
             objs.append(obj)
             if verbose and dt:
                 print(f"  {os.path.basename(obj)}: {dt:.1f}s", flush=True)
             if ptxas and err:
                 print(err)
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcublas", "-lcudart"]
+    if force or not os.path.exists(lib_path) or os.path.getmtime(lib_path) < max(
+            os.path.getmtime(o) for o in objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", lib_path, *objs, "-lcublas", "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
-    return LIB
+    return lib_path
 
 
 if __name__ == "__main__":
@@ -108,6 +114,9 @@ if __name__ == "__main__":
     ap.add_argument("-j", type=int, default=None)
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--ptxas", action="store_true")
+    ap.add_argument("--debug-bounds", action="store_true",
+                    help="build libgbx_eri_debug.so with every kernel store index-checked")
     a = ap.parse_args()
     t = time.time()
-    print(build(a.lmax, a.j, a.force, verbose=True, ptxas=a.ptxas), f"{time.time() - t:.1f}s")
+    print(build(a.lmax, a.j, a.force, verbose=True, ptxas=a.ptxas, debug=a.debug_bounds),
+          f"{time.time() - t:.1f}s")

@@ -88,6 +88,14 @@ struct Batch {
   double mix_skip = -1.0, mix_fp32 = -1.0;
   cudaGraph_t graph_m = nullptr;
   cudaGraphExec_t graph_exec_m = nullptr;
+  // multi-class queue form (gbx_batch_set_queue): the FP64 run's class kernels replaced by one
+  // persistent eri_queue launch that drains every block type's quartets from a single queue
+  bool use_queue = false;
+  void* d_qargs = nullptr;
+  QueueSeg* d_qsegs = nullptr;
+  unsigned long long* d_qcursor = nullptr;
+  QueuePlan qplan;
+  unsigned long long* d_fault = nullptr;  // debug builds: fault word of the bounds checks
 
   int alloc(void** p, size_t bytes, const char* what) {
     if (bytes == 0) bytes = 16;
@@ -283,11 +291,16 @@ static int build_batch(Batch& Bt, int n_mol, const int* mol_nshells, const int* 
   if ((s = Bt.upload(&Bt.d_rowinfo, rowinfo, "upload batch rowinfo"))) return s;
   if ((s = Bt.upload(&Bt.d_blocks, blocks, "upload batch block tables"))) return s;
   if ((s = Bt.upload(&Bt.d_row_first, row_first, "upload batch row offsets"))) return s;
+  if ((s = alloc_fault_word(&Bt.d_fault))) return s;
+  if (Bt.d_fault) Bt.allocs.push_back(Bt.d_fault);
   Bt.h_exp.resize(n_mol);
   for (int m = 0; m < n_mol; ++m) {
     const Basis& B = *Bt.mols[m];
     ExpandArgs e;
     memset(&e, 0, sizeof(e));
+    e.fault = Bt.d_fault;
+    e.out_len = B.nbf * B.nbf * B.nbf * B.nbf;
+    e.compact_len = (m + 1 < n_mol ? Bt.compact_off[m + 1] : Bt.compact_elems) - Bt.compact_off[m];
     e.n = B.nbf;
     e.nsh = (int)B.shells.size();
     e.notation = GBX_CHEMIST;
@@ -461,11 +474,75 @@ static int batch_mixed_lists(Batch& Bt, double skip, double fp32) {
   return GBX_OK;
 }
 
+// Arguments of block type k's class-kernel launches (FP64 work list, per-molecule stores).
+static EriLaunch type_launch(const Batch& Bt, int k) {
+  const BatchType& T = Bt.types[k];
+  EriLaunch a;
+  memset(&a, 0, sizeof(a));
+  a.pairs = Bt.d_pairs;
+  a.prims = Bt.d_prims;
+  a.shells = Bt.d_shells;
+  a.boys_tab = Bt.d_boys;
+  a.out = Bt.d_compact;
+  a.work = Bt.d_work;
+  a.work_off = T.work_off;
+  a.nwork = T.n;
+  a.mode = 0;
+  a.team = T.team;
+  a.variant = T.variant;
+  a.mol_base = T.d_base;
+  a.mol_ncols = T.d_ncols;
+  a.fault = Bt.d_fault;
+  a.out_len = Bt.compact_elems;
+  return a;
+}
+
+// The queue of the multi-class form, made on first use: the block types in launch order
+// (largest estimated cost first, so that the long quartets are drawn early), each a segment
+// with its class's programs.
+static int ensure_queue(Batch& Bt) {
+  if (Bt.d_qargs) return GBX_OK;
+  const int nseg = (int)Bt.order.size();
+  std::vector<EriLaunch> launches(nseg);
+  std::vector<int> progs(nseg);
+  std::vector<long long> counts(nseg);
+  for (int i = 0; i < nseg; ++i) {
+    const int k = Bt.order[i];
+    const BatchType& T = Bt.types[k];
+    launches[i] = type_launch(Bt, k);
+    progs[i] = coop_program(kPairClassL[T.cb][0], kPairClassL[T.cb][1], kPairClassL[T.ck][0],
+                            kPairClassL[T.ck][1]);
+    counts[i] = T.n;
+  }
+  std::vector<unsigned char> blob;
+  std::vector<QueueSeg> segs;
+  int s = queue_plan(launches.data(), progs.data(), counts.data(), nseg, blob, segs, Bt.qplan);
+  if (s) return s;
+  void* dargs = nullptr;
+  if ((s = Bt.alloc(&dargs, blob.size(), "cudaMalloc(queue arguments)"))) return s;
+  GBX_CUDA(cudaMemcpy(dargs, blob.data(), blob.size(), cudaMemcpyHostToDevice),
+           "upload queue arguments");
+  if ((s = Bt.upload(&Bt.d_qsegs, segs, "upload queue segments"))) return s;
+  if ((s = Bt.alloc((void**)&Bt.d_qcursor, sizeof(unsigned long long), "cudaMalloc(queue cursor)")))
+    return s;
+  Bt.d_qargs = dargs;
+  return GBX_OK;
+}
+
 // The launches of one batch run on stream `st` (class kernels on the auxiliary streams).
 // mixed: the lists of batch_mixed_lists, FP32 lists on the register kernel's FP32 path, and
 // the compact store cleared first when quartets were left out (their values are zero).
 static int enqueue_batch(Batch& Bt, cudaStream_t st, bool mixed = false) {
   const int nsm = num_sms_of(Bt.device);
+  if (Bt.use_queue && !mixed && !Bt.profile) {
+    // multi-class form: one persistent launch drains every block type, then the expansion
+    int s = ensure_queue(Bt);
+    if (s) return s;
+    GBX_CUDA(cudaMemsetAsync(Bt.d_qcursor, 0, sizeof(unsigned long long), st), "clear queue cursor");
+    if ((s = launch_queue(Bt.d_qargs, Bt.d_qsegs, Bt.d_qcursor, Bt.qplan, Bt.device, st))) return s;
+    return launch_expand_batch(Bt.device, Bt.d_exp, Bt.d_row_first, Bt.nmol, Bt.total_rows,
+                               Bt.max_row_bytes, st);
+  }
   if (mixed && Bt.mix_count[2] > 0)
     GBX_CUDA(cudaMemsetAsync(Bt.d_compact, 0, (size_t)Bt.compact_elems * sizeof(double), st),
              "clear batch compact store");
@@ -479,21 +556,7 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st, bool mixed = false) {
     const int k = Bt.order[i];
     const BatchType& T = Bt.types[k];
     if (Bt.profile) GBX_CUDA(cudaEventRecord(Bt.type_ev[i], st), "type event");
-    EriLaunch a;
-    memset(&a, 0, sizeof(a));
-    a.pairs = Bt.d_pairs;
-    a.prims = Bt.d_prims;
-    a.shells = Bt.d_shells;
-    a.boys_tab = Bt.d_boys;
-    a.out = Bt.d_compact;
-    a.work = Bt.d_work;
-    a.work_off = T.work_off;
-    a.nwork = T.n;
-    a.mode = 0;
-    a.team = T.team;
-    a.variant = T.variant;
-    a.mol_base = T.d_base;
-    a.mol_ncols = T.d_ncols;
+    EriLaunch a = type_launch(Bt, k);
     a.ticket = tickets ? Bt.d_tickets + 2 * k : nullptr;
     cudaStream_t ts = Bt.profile ? st : Bt.aux[i % Bt.aux.size()];
     if (mixed) {
@@ -532,12 +595,14 @@ static int enqueue_batch(Batch& Bt, cudaStream_t st, bool mixed = false) {
 // mixed: thresholds (skip, fp32) of the mixed form, nullptr for the FP64 form.
 static int run_batch(Batch& Bt, int notation, double* const* outs, cudaStream_t caller,
                      const double* mixed = nullptr) {
+  NvtxRange range("gbx batch run");
   for (int m = 0; m < Bt.nmol; ++m)
     if (!outs[m]) return set_error(GBX_ERR_INVALID, "output of molecule %d is null", m);
   bool changed = Bt.exp_dirty;
   for (int m = 0; m < Bt.nmol; ++m) {
     if (Bt.h_exp[m].out != outs[m] || Bt.h_exp[m].notation != notation) changed = true;
     Bt.h_exp[m].out = outs[m];
+    Bt.h_exp[m].out_lo = outs[m];
     Bt.h_exp[m].notation = notation;
   }
   GBX_CUDA(cudaEventRecord(Bt.ev_in, caller), "record caller");
@@ -641,6 +706,16 @@ static void batch_drop_graph(Batch& B) {
   batch_drop_mixed_graph(B);
 }
 
+int gbx_batch_set_queue(gbx_batch* b, int on) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_batch_set_queue: null batch");
+  Batch& B = *b->impl;
+  if (B.use_queue != (on != 0)) {
+    B.use_queue = on != 0;
+    batch_drop_graph(B);
+  }
+  return GBX_OK;
+}
+
 int gbx_batch_num_types(const gbx_batch* b, int* n) {
   if (!b || !n) return set_error(GBX_ERR_INVALID, "gbx_batch_num_types: null argument");
   *n = (int)b->impl->types.size();
@@ -727,7 +802,8 @@ int gbx_batch_run(gbx_batch* b, int notation, double* const* outs, void* stream)
     return set_error(GBX_ERR_INVALID, "notation must be GBX_CHEMIST or GBX_PHYSICIST");
   Batch& B = *b->impl;
   DeviceGuardLite g(B.device);
-  return run_batch(B, notation, outs, (cudaStream_t)stream);
+  const int s = run_batch(B, notation, outs, (cudaStream_t)stream);
+  return s ? s : check_bounds_fault(B.d_fault, (cudaStream_t)stream, "gbx_batch_run");
 }
 
 int gbx_batch_run_mixed(gbx_batch* b, int notation, double skip, double fp32,
@@ -740,7 +816,8 @@ int gbx_batch_run_mixed(gbx_batch* b, int notation, double skip, double fp32,
   Batch& B = *b->impl;
   DeviceGuardLite g(B.device);
   const double th[2] = {skip, fp32};
-  return run_batch(B, notation, outs, (cudaStream_t)stream, th);
+  const int s = run_batch(B, notation, outs, (cudaStream_t)stream, th);
+  return s ? s : check_bounds_fault(B.d_fault, (cudaStream_t)stream, "gbx_batch_run_mixed");
 }
 
 int gbx_batch_mixed_counts(const gbx_batch* b, int64_t* n_fp64, int64_t* n_fp32,

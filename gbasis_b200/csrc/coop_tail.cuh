@@ -32,7 +32,7 @@ constexpr long long kCoopMaxSmem = 227 * 1024;
 // staged programs: shared memory, not registers, is what limits these kernels' occupancy (a
 // class with f shells took 125 KB per 4-warp CTA with the largest chunks: 4 warps per SM).
 inline int coop_plan(const CoopMeta& M, long long phase_a, CoopArgs& A, size_t& smem, int& wpc,
-                     int max_warps_regs = 16) {
+                     int max_warps_regs = 16, bool allow_staged = true) {
   const int NCD = ncart(M.lc) * ncart(M.ld), NAB = ncart(M.la) * ncart(M.lb);
   const int NENF = M.NE * M.NF;
   const long long warp_cap = 48 * 1024 / 8;
@@ -53,7 +53,7 @@ inline int coop_plan(const CoopMeta& M, long long phase_a, CoopArgs& A, size_t& 
       const long long per_warp = size_for(R, Cc);
       if (per_warp > warp_cap && !(R == 1 && Cc == 1)) continue;
       for (int staged = 1; staged >= 0; --staged) {
-        if (staged && prog_bytes > 32 * 1024) continue;
+        if (staged && (!allow_staged || prog_bytes > 32 * 1024)) continue;
         const long long prog = staged ? (prog_bytes + 15) / 16 * 16 : 0;
         for (int w = 1; w <= 4; ++w) {
           const long long cta = prog + extra + (long long)w * per_warp * 8;
@@ -258,7 +258,6 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
   long long bbase, bcols;
   block_dest(a, P, bbase, bcols);
   const bool tr = quartet_transposed(P, Q);  // values stored at [ket row][bra column]
-  double* __restrict__ dst = a.out + bbase;
   for (int c0 = 0; c0 < ncol; c0 += A.Cc) {
     const int cc = min(A.Cc, ncol - c0);
     for (int i = lane; i < cc * M.NE; i += 32) {
@@ -326,8 +325,8 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
           for (int i = 0; i < nab; ++i) s = fma(OB[c * NAB + i], DAB[i], s);
           s *= ((P.shA != P.shB) ? 2.0 : 1.0) * sC.scl[uc] * sD.scl[ud];
           const long long fc = sC.func_off + sC.pos[uc], fd = sD.func_off + sD.pos[ud];
-          atomicAdd(a.J + fc * a.nbf + fd, s);
-          if (Q.shA != Q.shB) atomicAdd(a.J + fd * a.nbf + fc, s);
+          j_add(a, fc * a.nbf + fd, s);
+          if (Q.shA != Q.shB) j_add(a, fd * a.nbf + fc, s);
         }
       }
       __syncwarp();
@@ -346,7 +345,7 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
                        sD.scl[ud];
       const long long rab = (long long)P.fo + sA.pos[ua] * nBo + sB.pos[ub];
       const long long rcd = (long long)Q.fo + sC.pos[uc] * nDo + sD.pos[ud];
-      dst[tr ? rcd * bcols + rab : rab * bcols + rcd] = v;
+      out_store(a, bbase + (tr ? rcd * bcols + rab : rab * bcols + rcd), v);
     }
     __syncwarp();
   }
@@ -360,8 +359,8 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
       const int ua = i / nBi, ub = i - ua * nBi;
       const long long fa = sA.func_off + sA.pos[ua], fbn = sB.func_off + sB.pos[ub];
       const double s = VAB[i] * fk * sA.scl[ua] * sB.scl[ub];
-      atomicAdd(a.J + fa * a.nbf + fbn, s);
-      if (P.shA != P.shB) atomicAdd(a.J + fbn * a.nbf + fa, s);
+      j_add(a, fa * a.nbf + fbn, s);
+      if (P.shA != P.shB) j_add(a, fbn * a.nbf + fa, s);
     }
   }
   __syncwarp();

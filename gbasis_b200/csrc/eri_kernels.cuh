@@ -215,8 +215,8 @@ __device__ __forceinline__ void coulomb_epilogue(const EriLaunch& a, int2 pq, co
         w[c] = fma(x, dab, w[c]);
       }
       s *= fk * sab;
-      atomicAdd(a.J + fa * n + fbn, s);
-      if (P.shA != P.shB) atomicAdd(a.J + fbn * n + fa, s);
+      j_add(a, fa * n + fbn, s);
+      if (P.shA != P.shB) j_add(a, fbn * n + fa, s);
     }
   }
   if (!swap) return;
@@ -228,8 +228,8 @@ __device__ __forceinline__ void coulomb_epilogue(const EriLaunch& a, int2 pq, co
       if (id >= nDi) break;
       const long long fc = sC.func_off + sC.pos[ic], fd = sD.func_off + sD.pos[id];
       const double s = w[ic * ND + id] * fb * sC.scl[ic] * sD.scl[id];
-      atomicAdd(a.J + fc * n + fd, s);
-      if (Q.shA != Q.shB) atomicAdd(a.J + fd * n + fc, s);
+      j_add(a, fc * n + fd, s);
+      if (Q.shA != Q.shB) j_add(a, fd * n + fc, s);
     }
   }
 }
@@ -390,7 +390,6 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
     // (quartet_transposed: a diagonal-block quartet run from its lower pair)
     auto store = [&](auto transposed) {
       constexpr bool TR = decltype(transposed)::value;
-      double* __restrict__ dst = a.out + bbase;
 #pragma unroll
       for (int ia = 0; ia < NCA; ++ia) {
         if (ia >= nAi) break;
@@ -410,8 +409,8 @@ __global__ void __launch_bounds__(kEriThreads, eri_min_blocks(LA, LB, LC, LD))
             for (int id = 0; id < NCD; ++id) {
               if (id >= nDi) break;
               const long long rcd = rc + sD.pos[id];
-              dst[TR ? rcd * bcols + rab : rab * bcols + rcd] =
-                  out[((ia * NCB + ib) * NCC + ic) * NCD + id] * fabc * sD.scl[id];
+              out_store(a, bbase + (TR ? rcd * bcols + rab : rab * bcols + rcd),
+                        out[((ia * NCB + ib) * NCC + ic) * NCD + id] * fabc * sD.scl[id]);
             }
           }
         }

@@ -142,6 +142,10 @@ struct EriLaunch {
   // work.  nullptr, and in the light-class register kernel: the static order, quartet w to
   // warp w mod (warps in the grid).
   unsigned long long* ticket;
+  // debug builds (GBX_DEBUG_BOUNDS): fault word of the call and the length of `out` in
+  // elements (mode 0 stores); nullptr: this launch's stores are not checked
+  unsigned long long* fault;
+  long long out_len;
 };
 
 // Next work ticket of a warp (every lane of the warp calls it; lane 0 draws).
@@ -149,6 +153,51 @@ __device__ __forceinline__ long long warp_ticket(unsigned long long* t, int lane
   unsigned long long v = 0;
   if (lane == 0) v = atomicAdd(t, 1ull);
   return (long long)__shfl_sync(0xffffffffu, v, 0);
+}
+
+// ----------------------------------------------------------------- debug bounds checks
+// Builds compiled with -DGBX_DEBUG_BOUNDS=1 (libgbx_eri_debug.so) check the index of every
+// store of the class kernels, the work-list build, the zero fill, the expansions and the J / K
+// scatter, and of the expansions' compact-store reads, against the array it addresses.  An
+// index outside it is recorded in the call's fault word (the first one: site in the top byte,
+// index below) and the access is skipped; the entry point then returns GBX_ERR_INVALID naming
+// both.  Release builds compile the checks away.  Launches given no fault word are unchecked.
+#ifndef GBX_DEBUG_BOUNDS
+#define GBX_DEBUG_BOUNDS 0
+#endif
+enum BoundsSite : int {
+  kSiteClassStore = 1,   // class kernel store into the compact store
+  kSiteWorkList = 2,     // work-list build (FP64, FP32 and zero lists)
+  kSiteZeroFill = 3,     // zero_quartets
+  kSiteExpand = 4,       // expansion store into the N^4 tensor (or a host-copy slab)
+  kSiteCompactRead = 5,  // expansion / J-K read of the compact store
+  kSiteJK = 6,           // Coulomb / exchange matrix scatter
+};
+
+__device__ __forceinline__ bool gbx_in_bounds(unsigned long long* fault, int site, long long i,
+                                              long long n) {
+#if GBX_DEBUG_BOUNDS
+  if (!fault || (i >= 0 && i < n)) return true;
+  const unsigned long long idx = i < 0 ? 0x00ffffffffffffffull : (unsigned long long)i;
+  atomicCAS(fault, 0ull, ((unsigned long long)site << 56) | (idx & 0x00ffffffffffffffull));
+  return false;
+#else
+  (void)fault;
+  (void)site;
+  (void)i;
+  (void)n;
+  return true;
+#endif
+}
+
+// a.out[i] = v: a class kernel's store into the compact store.
+__device__ __forceinline__ void out_store(const EriLaunch& a, long long i, double v) {
+  if (gbx_in_bounds(a.fault, kSiteClassStore, i, a.out_len)) a.out[i] = v;
+}
+
+// J[i] += v: a Coulomb-mode contribution (J is nbf x nbf).
+__device__ __forceinline__ void j_add(const EriLaunch& a, long long i, double v) {
+  if (gbx_in_bounds(a.fault, kSiteJK, i, a.nbf * a.nbf)) atomicAdd(a.J + i, v);
 }
 
 // Destination block of a quartet whose bra pair is P.

@@ -135,7 +135,10 @@ def program(la, lb, lc, ld):
                 kins=kins, klv=klv, nK=knxt, kfin=kfin, bins=bins, blv=blv, nB=bnxt, bfin=bfin)
 
 
-def emit(classes, path):
+def emit(classes, path, n_heavy=None):
+    """Programs of ``classes``; the first ``n_heavy`` (default: all) are the heavy classes that
+    the cooperative kernels run per class block; the rest serve the multi-class queue kernel."""
+    n_heavy = len(classes) if n_heavy is None else n_heavy
     ins, lv, idx = [], [], []
     metas = []
     for c in classes:
@@ -174,6 +177,7 @@ def emit(classes, path):
     lines.append(f"__device__ const int kCoopLv[{max(1, len(lv))}] = {{{', '.join(map(str, lv)) or '0'}}};")
     lines.append(f"__device__ const short kCoopIdx[{max(1, len(idx))}] = {{{', '.join(map(str, idx)) or '0'}}};")
     lines.append(f"const int kCoopNumClasses = {len(metas)};")
+    lines.append(f"const int kCoopNumHeavy = {n_heavy};")
     lines.append("const CoopMeta kCoopMeta[] = {")
     for m in metas:
         la, lb, lc, ld = m["cls"]

@@ -409,7 +409,9 @@ def emit_sources(outdir, lmax):
     # the point-charge kernel uses the (ab|ss) structs of every pair class, heavy ones included
     one_e = [(la, lb, 0, 0) for la in range(lmax + 1) for lb in range(lmax + 1)]
     put("eri_gen.cuh", emit_all(lmax, light + [c for c in one_e if c not in light]))
-    gen_coop.emit(heavy, os.path.join(outdir, "coop_programs.cuh"))
+    # heavy classes first (their cooperative kernels index the table by position), then the
+    # light classes, whose programs only the multi-class queue kernel runs
+    gen_coop.emit(heavy + light, os.path.join(outdir, "coop_programs.cuh"), n_heavy=len(heavy))
     files = []
     # spread the light classes over translation units of similar compile cost (code size)
     nbins = 12

@@ -292,7 +292,6 @@ __device__ __forceinline__ void lines_tail(const EriLaunch& a, const double* ACC
   // strides of the bra and ket pair-function indices (transposed: quartet_transposed)
   const bool tr = quartet_transposed(P, Q);
   const long long sbra = tr ? 1 : bcols, sket = tr ? bcols : 1;
-  double* __restrict__ dst = a.out + bbase;
   const long long nBo = sB.nout, nDo = sD.nout;
   double mx = 0.0;
   for (int k = lane; k < ncol; k += 32) {
@@ -311,7 +310,7 @@ __device__ __forceinline__ void lines_tail(const EriLaunch& a, const double* ACC
     if (LB >= 2 && sB.sph) sph_axis<LB, NCA, 1>(o);
     if (LA >= 2 && sA.sph) sph_axis<LA, 1, NCB>(o);
     const double fcd = sC.scl[uc] * sD.scl[ud];
-    double* __restrict__ col = dst + ((long long)Q.fo + sC.pos[uc] * nDo + sD.pos[ud]) * sket;
+    const long long col = bbase + ((long long)Q.fo + sC.pos[uc] * nDo + sD.pos[ud]) * sket;
 #pragma unroll
     for (int ia = 0; ia < NCA; ++ia) {
       if (ia >= nAi) break;
@@ -320,7 +319,7 @@ __device__ __forceinline__ void lines_tail(const EriLaunch& a, const double* ACC
 #pragma unroll
       for (int ib = 0; ib < NCB; ++ib) {
         if (ib >= nBi) break;
-        col[(ra + sB.pos[ib]) * sbra] = o[ia * NCB + ib] * fa * sB.scl[ib];
+        out_store(a, col + (ra + sB.pos[ib]) * sbra, o[ia * NCB + ib] * fa * sB.scl[ib]);
       }
     }
   }
@@ -550,8 +549,8 @@ __device__ __forceinline__ void split_tail(const EriLaunch& a, double* ACC,
       }
       if (s.bra != s.ket) {
         const double w = scd * ((s.shA != s.shB) ? 2.0 : 1.0) * fcd;
-        atomicAdd(a.J + fc * n + fd, w);
-        if (s.shC != s.shD) atomicAdd(a.J + fd * n + fc, w);
+        j_add(a, fc * n + fd, w);
+        if (s.shC != s.shD) j_add(a, fd * n + fc, w);
       }
       continue;
     }
@@ -566,8 +565,7 @@ __device__ __forceinline__ void split_tail(const EriLaunch& a, double* ACC,
     const long long nBo = sB.nout, nDo = sD.nout;
     const double fcd = sC.scl[uc] * sD.scl[ud];
     const long long sbra = s.tr ? 1 : bcols, sket = s.tr ? bcols : 1;
-    double* __restrict__ col =
-        a.out + bbase + ((long long)s.qfo + sC.pos[uc] * nDo + sD.pos[ud]) * sket;
+    const long long col = bbase + ((long long)s.qfo + sC.pos[uc] * nDo + sD.pos[ud]) * sket;
 #pragma unroll
     for (int ia = 0; ia < NCA; ++ia) {
       if (ia >= nAi) break;
@@ -576,7 +574,7 @@ __device__ __forceinline__ void split_tail(const EriLaunch& a, double* ACC,
 #pragma unroll
       for (int ib = 0; ib < NCB; ++ib) {
         if (ib >= nBi) break;
-        col[(ra + sB.pos[ib]) * sbra] = o[ia * NCB + ib] * fa * sB.scl[ib];
+        out_store(a, col + (ra + sB.pos[ib]) * sbra, o[ia * NCB + ib] * fa * sB.scl[ib]);
       }
     }
   }
@@ -596,8 +594,8 @@ __device__ __forceinline__ void split_tail(const EriLaunch& a, double* ACC,
       if (ia >= internal_count(sA) || ib >= internal_count(sB)) continue;
       const long long fa = sA.func_off + sA.pos[ia], fb = sB.func_off + sB.pos[ib];
       const double v = JAB[t] * ((s.shC != s.shD) ? 2.0 : 1.0) * sA.scl[ia] * sB.scl[ib];
-      atomicAdd(a.J + fa * n + fb, v);
-      if (s.shA != s.shB) atomicAdd(a.J + fb * n + fa, v);
+      j_add(a, fa * n + fb, v);
+      if (s.shA != s.shB) j_add(a, fb * n + fa, v);
     }
   }
 }

@@ -122,7 +122,7 @@ __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* _
   const int2 cm = cta_map[blockIdx.x];
   const BuildBlock B = bb[cm.x];
   const long long t = (long long)cm.y + threadIdx.x;
-  bool pass = false, fp32 = false;
+  bool pass = false, fp32 = false, zero = false;
   int p = 0, q = 0;
   if (t < B.ncand) {
     long long pl, ql;
@@ -142,7 +142,10 @@ __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* _
       // mixed form: bound of the final values (Schwarz bound times the largest output scale
       // of each shell) decides skip (< skip), FP32 (< fp32) or FP64
       const double bnd = mp.qm[p] * mp.qm[q];
-      if (bnd < mp.skip) pass = false;
+      if (bnd < mp.skip) {
+        zero = pass && mp.zero_work != nullptr;  // listed for zero_quartets
+        pass = false;
+      }
       fp32 = pass && B.fp32_ok && (!mp.fp32_on || mp.fp32_on[B.blk]) && bnd < mp.fp32;
     }
   }
@@ -162,9 +165,52 @@ __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* _
   base = __shfl_sync(0xffffffffu, base, 0);
   base32 = __shfl_sync(0xffffffffu, base32, 0);
   const unsigned below = (1u << lane) - 1u;
-  if (p64) work[B.work_off + base + __popc(mask & below)] = make_int2(p, q);
-  if (fp32)  // FP32 quartets fill the block's slots from the end
-    work[B.work_off + B.ncand - 1 - (base32 + __popc(mask32 & below))] = make_int2(p, q);
+  if (p64) {
+    const long long i = base + __popc(mask & below);
+    if (gbx_in_bounds(mp.fault, kSiteWorkList, i, B.ncand)) work[B.work_off + i] = make_int2(p, q);
+  }
+  if (fp32) {  // FP32 quartets fill the block's slots from the end
+    const long long i = B.ncand - 1 - (base32 + __popc(mask32 & below));
+    if (gbx_in_bounds(mp.fault, kSiteWorkList, i, B.ncand)) work[B.work_off + i] = make_int2(p, q);
+  }
+  if (mp.zero_work) {
+    // left-out quartets in their listed orientation (bra pair p of the block's bra class)
+    const unsigned maskz = __ballot_sync(0xffffffffu, zero);
+    int basez = 0;
+    if (lane == 0 && maskz) basez = atomicAdd(mp.zero_count, __popc(maskz));
+    basez = __shfl_sync(0xffffffffu, basez, 0);
+    const long long iz = (long long)basez + __popc(maskz & below);
+    if (zero && iz < mp.zero_cap) mp.zero_work[iz] = make_int2(p, q);
+    else if (zero) gbx_in_bounds(mp.fault, kSiteWorkList, iz, mp.zero_cap);  // recorded
+  }
+}
+
+// Mixed form: zeros in the compact store for the left-out quartets of a call (those whose
+// final-value bound is below the skip threshold), in place of clearing the whole store.  A
+// warp per quartet clears its entries of the block matrix: rows P.fo .. P.fo + nout(A) nout(B)
+// - 1 (the bra pair's functions) by the ket pair's columns, where a computed quartet of the
+// same orientation would have stored them.
+__global__ void zero_quartets(const int2* __restrict__ list, const int* __restrict__ count,
+                              long long cap, const PairDev* __restrict__ pairs,
+                              const ShellDev* __restrict__ shells,
+                              const BlockDev* __restrict__ blocks, double* __restrict__ out,
+                              long long out_len, unsigned long long* fault) {
+  const long long n = min((long long)*count, cap);
+  const int lane = threadIdx.x & 31;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += nw) {
+    const int2 pq = list[w];
+    const PairDev P = pairs[pq.x];
+    const PairDev Q = pairs[pq.y];
+    const BlockDev b = blocks[P.cls * kNumPairClasses + Q.cls];
+    const int nr = shells[P.shA].nout * P.nB, nc = shells[Q.shA].nout * Q.nB;
+    const long long first = b.base + (long long)P.fo * b.ncols + Q.fo;
+    for (int i = lane; i < nr * nc; i += 32) {
+      const int r = i / nc, c = i - r * nc;
+      const long long at = first + (long long)r * b.ncols + c;
+      if (gbx_in_bounds(fault, kSiteZeroFill, at, out_len)) out[at] = 0.0;
+    }
+  }
 }
 
 // ------------------------------------------------------------------- K6
@@ -181,6 +227,15 @@ __device__ __forceinline__ long long pair_row(const ExpandArgs& e, int s1, int c
 __device__ __forceinline__ int fk_cls(long long k) { return (int)(k >> 56); }
 __device__ __forceinline__ int fk_loc(long long k) { return (int)((k >> 32) & 0xffffff); }
 __device__ __forceinline__ long long fk_row(long long k) { return k & 0xffffffffLL; }
+
+// Debug builds: the expansion's destination p within the launch's output range, and a
+// compact-store read index within the store.
+__device__ __forceinline__ bool dst_ok(const ExpandArgs& e, const double* p) {
+  return gbx_in_bounds(e.fault, kSiteExpand, (long long)(p - e.out_lo), e.out_len);
+}
+__device__ __forceinline__ bool compact_ok(const ExpandArgs& e, long long i) {
+  return gbx_in_bounds(e.fault, kSiteCompactRead, i, e.compact_len);
+}
 
 __global__ void __launch_bounds__(256) expand_full(const ExpandArgs e) {
   __shared__ long long s_base[kNumPairClasses * kNumPairClasses];
@@ -222,7 +277,7 @@ __global__ void __launch_bounds__(256) expand_full(const ExpandArgs e) {
           const int t = cq * kNumPairClasses + cp;
           off = s_base[t] + (long long)rowq * s_ncols[t] + rowp;
         }
-        orow[d] = __ldg(e.compact + off);
+        if (compact_ok(e, off) && dst_ok(e, orow + d)) orow[d] = __ldg(e.compact + off);
       }
     }
   }
@@ -252,14 +307,15 @@ __device__ __forceinline__ void stage_row(const ExpandArgs& e, long long r, int 
       // a row of block (X, Y) (unit stride) or a column of block (Y, X) (stride = columns);
       // four loads in flight per thread
       const BlockDev b = X > Y ? e.blocks[X * kNumPairClasses + Y] : e.blocks[Y * kNumPairClasses + X];
-      const double* __restrict__ src = e.compact + b.base + (X > Y ? rho * b.ncols : rho);
+      const long long s0 = b.base + (X > Y ? rho * b.ncols : rho);
+      const double* __restrict__ src = e.compact + s0;
       const long long stride = X > Y ? 1 : b.ncols;
       for (long long j0 = tid; j0 < ny; j0 += 4LL * nt) {
         double v[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           const long long j = j0 + (long long)k * nt;
-          v[k] = j < ny ? __ldg(src + j * stride) : 0.0;
+          v[k] = (j < ny && compact_ok(e, s0 + j * stride)) ? __ldg(src + j * stride) : 0.0;
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -272,7 +328,8 @@ __device__ __forceinline__ void stage_row(const ExpandArgs& e, long long r, int 
       const double* __restrict__ blk = e.compact + b.base;
       for (long long j = tid; j < ny; j += nt) {
         const int lj = __ldg(&e.rowinfo[y0 + j].w);
-        s_row[y0 + j] = __ldg(lj <= lr ? blk + rho * b.ncols + j : blk + j * b.ncols + rho);
+        const long long at = lj <= lr ? rho * b.ncols + j : j * b.ncols + rho;
+        s_row[y0 + j] = compact_ok(e, b.base + at) ? __ldg(blk + at) : 0.0;
       }
     }
   }
@@ -304,8 +361,8 @@ __device__ __forceinline__ void write_plane(const ExpandArgs& e, const double* _
         const unsigned t = t0 + k * nt;
         if (t < n2) {
           const double v = s_row[g[k]];
-          __stcs(dst + t, v);
-          if (mir) __stcs(mir + t, v);
+          if (dst_ok(e, dst + t)) __stcs(dst + t, v);
+          if (mir && dst_ok(e, mir + t)) __stcs(mir + t, v);
         }
       }
     }
@@ -328,8 +385,8 @@ __device__ __forceinline__ void write_plane(const ExpandArgs& e, const double* _
           const int d = d0 + 32 * k;
           if (d < n) {
             const double v = s_row[g[k]];
-            __stcs(drow + d, v);
-            if (mrow) __stcs(mrow + d, v);
+            if (dst_ok(e, drow + d)) __stcs(drow + d, v);
+            if (mrow && dst_ok(e, mrow + d)) __stcs(mrow + d, v);
           }
         }
       }
@@ -380,10 +437,12 @@ __device__ __forceinline__ double compact_at(const ExpandArgs& e, int X, long lo
   const int lq = __ldg(&e.rowinfo[q].w);
   if (X > Y || (X == Y && lp >= lq)) {
     const BlockDev bd = e.blocks[X * kNumPairClasses + Y];
-    return __ldg(e.compact + bd.base + rp * bd.ncols + rq);
+    const long long at = bd.base + rp * bd.ncols + rq;
+    return compact_ok(e, at) ? __ldg(e.compact + at) : 0.0;
   }
   const BlockDev bd = e.blocks[Y * kNumPairClasses + X];
-  return __ldg(e.compact + bd.base + rq * bd.ncols + rp);
+  const long long at = bd.base + rq * bd.ncols + rp;
+  return compact_ok(e, at) ? __ldg(e.compact + at) : 0.0;
 }
 
 // Coulomb and exchange matrices from the compact store.  Row r of M (the pair function of the
@@ -432,8 +491,10 @@ __global__ void __launch_bounds__(512) jk_rows(const ExpandArgs e, const double*
         ky += __shfl_xor_sync(0xffffffffu, ky, o);
       }
       if (lane == 0) {
-        atomicAdd(K + (long long)ri.x * n + c, kx);
-        if (ri.z) atomicAdd(K + (long long)ri.y * n + c, ky);
+        const long long n2 = (long long)n * n;
+        const long long kx_at = (long long)ri.x * n + c, ky_at = (long long)ri.y * n + c;
+        if (gbx_in_bounds(e.fault, kSiteJK, kx_at, n2)) atomicAdd(K + kx_at, kx);
+        if (ri.z && gbx_in_bounds(e.fault, kSiteJK, ky_at, n2)) atomicAdd(K + ky_at, ky);
       }
     }
     for (int o = 16; o > 0; o >>= 1) jp += __shfl_xor_sync(0xffffffffu, jp, o);
@@ -442,8 +503,10 @@ __global__ void __launch_bounds__(512) jk_rows(const ExpandArgs e, const double*
     if (threadIdx.x == 0) {
       double t = 0.0;
       for (int w = 0; w < nw; ++w) t += s_j[w];
-      J[(long long)ri.x * n + ri.y] = t;
-      if (ri.z) J[(long long)ri.y * n + ri.x] = t;
+      const long long n2 = (long long)n * n;
+      const long long j0 = (long long)ri.x * n + ri.y, j1 = (long long)ri.y * n + ri.x;
+      if (gbx_in_bounds(e.fault, kSiteJK, j0, n2)) J[j0] = t;
+      if (ri.z && gbx_in_bounds(e.fault, kSiteJK, j1, n2)) J[j1] = t;
     }
   }
 }
@@ -469,7 +532,7 @@ __global__ void gather_unique(const ExpandArgs e, const long long* __restrict__ 
     const BlockDev bd = e.blocks[Y * kNumPairClasses + X];
     off = bd.base + rq * bd.ncols + rp;
   }
-  out[i] = e.compact[off];
+  out[i] = compact_ok(e, off) ? e.compact[off] : 0.0;
 }
 
 // Batch form of the row-staged expansion: molecule m's pair-function rows are the global rows
@@ -528,6 +591,7 @@ static int num_sms(int device) {
 }
 
 int upload_basis(Basis& B) {
+  NvtxRange range("gbx upload basis");
   const int n = (int)B.shells.size();
   const int np = (int)B.pairs.size();
   int s;
@@ -598,6 +662,11 @@ int upload_basis(Basis& B) {
   if ((s = B.alloc((void**)&B.d_q, np * sizeof(double), "cudaMalloc(q)"))) return s;
   if ((s = B.alloc((void**)&B.d_qscreen, np * sizeof(double), "cudaMalloc(qscreen)"))) return s;
   if ((s = boys_table(B.device, &B.d_boys))) return s;
+#if GBX_DEBUG_BOUNDS
+  if ((s = B.alloc((void**)&B.d_fault, sizeof(unsigned long long), "cudaMalloc(fault word)")))
+    return s;
+  GBX_CUDA(cudaMemset(B.d_fault, 0, sizeof(unsigned long long)), "clear fault word");
+#endif
   GBX_CUDA(cudaDeviceSynchronize(), "basis upload");
   return GBX_OK;
 }
@@ -688,6 +757,7 @@ static int class_dims(int cls, int& la, int& lb) {
 
 int ensure_schwarz(Basis& B, cudaStream_t st) {
   if (B.schwarz_ready) return GBX_OK;
+  NvtxRange range("gbx Schwarz bounds");
   const int np = (int)B.pairs.size();
   std::vector<int2> diag(np);
   for (int p = 0; p < np; ++p) diag[p] = make_int2(p, p);
@@ -797,6 +867,7 @@ __global__ void diagonal_block_bounds(const PairDev* __restrict__ pairs, int npa
 
 static int ensure_mixed_bounds(Basis& B, cudaStream_t st) {
   if (B.mixed_ready) return GBX_OK;
+  NvtxRange range("gbx mixed-form bounds");
   int s;
   const int np = (int)B.pairs.size();
   if (!B.d_qmixed && (s = B.alloc((void**)&B.d_qmixed, np * sizeof(double), "cudaMalloc(qmixed)")))
@@ -929,7 +1000,7 @@ static int ensure_mixed_counts(Basis& B, double skip, double fp32) {
                                       : 0;
     // an FP32 list pays for its own launch only when it holds a share of the block; the
     // quartets of a smaller one stay in the FP64 list
-    on[k] = B.mix_n32[k] >= kMinFp32List && B.mix_n32[k] * 20 >= h.ncand;
+    on[k] = B.mix_n32[k] >= B.fp32_min && B.mix_n32[k] * B.fp32_share >= h.ncand;
     if (!on[k]) B.mix_n32[k] = 0;
   }
   if (!B.d_fp32_on && B.alloc((void**)&B.d_fp32_on, nblk * sizeof(int), "cudaMalloc(fp32 flags)"))
@@ -942,6 +1013,7 @@ static int ensure_mixed_counts(Basis& B, double skip, double fp32) {
 }
 
 int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32) {
+  NvtxRange range("gbx work list and class kernels");
   int s;
   const bool mixed = skip > 0.0 || fp32 > 0.0;
   if (mixed && B.potential)
@@ -961,13 +1033,35 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
   long long left_out = 0;
   if (mixed)
     for (long long v : B.mix_nskip) left_out += v;
-  if (tau > 0.0 || left_out > 0) {
+  // the mixed form's left-out quartets (at most left_out: the host counts bound the device's)
+  // are listed by the work-list build and zeroed by zero_quartets, so that only their entries
+  // of the store are written
+  const bool zero_list = mixed && tau <= 0.0 && left_out > 0;
+  if (zero_list) {
+    if (B.zero_cap < left_out) {
+      if (B.d_zero_work) B.release(B.d_zero_work);
+      B.d_zero_work = nullptr;
+      B.zero_cap = 0;
+      if ((s = B.alloc((void**)&B.d_zero_work, (size_t)left_out * sizeof(int2),
+                       "cudaMalloc(zero list)")))
+        return s;
+      B.zero_cap = left_out;
+    }
+    if (!B.d_zero_count &&
+        (s = B.alloc((void**)&B.d_zero_count, sizeof(int), "cudaMalloc(zero count)")))
+      return s;
+    GBX_CUDA(cudaMemsetAsync(B.d_zero_count, 0, sizeof(int), st), "clear zero count");
+  }
+  if (tau > 0.0 || (left_out > 0 && !zero_list)) {
     // screened-out quartets are zero in the output: clear the store first
     GBX_CUDA(cudaMemsetAsync(B.d_compact, 0, B.compact_elems * sizeof(double), st),
              "clear compact store");
   }
+  B.last_mixed = mixed;
   const MixedParams mp{B.d_qmixed, skip, fp32, mixed ? B.d_counts32 : nullptr,
-                       mixed ? B.d_fp32_on : nullptr};
+                       mixed ? B.d_fp32_on : nullptr, zero_list ? B.d_zero_work : nullptr,
+                       zero_list ? B.d_zero_count : nullptr, zero_list ? B.zero_cap : 0,
+                       B.d_fault};
   if (B.profiling) cudaEventRecord(B.ev[0], st);
   build_work<<<B.n_cta_build, 256, 0, st>>>(B.d_cta_map, (const BuildBlock*)B.d_build_blocks,
                                             B.d_qscreen, tau, B.d_work, B.d_counts, mp,
@@ -987,6 +1081,15 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
     GBX_CUDA(cudaEventRecord(B.fork, st), "fork");
     for (int j = 0; j < nstreams; ++j) GBX_CUDA(cudaStreamWaitEvent(B.aux[j], B.fork, 0), "fork wait");
   }
+  if (zero_list) {
+    // on the caller's stream, beside the class blocks (disjoint entries of the store)
+    const int zgrid = (int)std::max<long long>(
+        1, std::min<long long>((B.zero_cap + 7) / 8, (long long)nsm * 8));
+    zero_quartets<<<zgrid, 256, 0, st>>>(B.d_zero_work, B.d_zero_count, B.zero_cap, B.d_pairs,
+                                         B.d_shells, B.d_blocks, B.d_compact, B.compact_elems,
+                                         B.d_fault);
+    GBX_CUDA(cudaGetLastError(), "zero_quartets launch");
+  }
   for (int i = 0; i < nblk; ++i) {
     const int k = B.launch_order.empty() ? i : B.launch_order[i];
     const cudaStream_t bs = nstreams ? B.aux[i % nstreams] : st;
@@ -1002,6 +1105,8 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
     a.base = h.dev.base;
     a.ncols = h.dev.ncols;
     a.mode = 0;
+    a.fault = B.d_fault;
+    a.out_len = B.compact_elems;
     a.team = h.team;
     a.variant = h.variant;
     a.potential = B.potential;
@@ -1015,14 +1120,15 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
         1, std::min<long long>((n64 * h.team + 127) / 128, (long long)nsm * h.ctas_per_sm));
     if (per_block) cudaEventRecord(B.blk_ev[i], st);
     if ((s = launch_class(la, lb, lc, ld, a, grid, bs))) return s;
-    if (n32 > 0) {  // the block's FP32 list
+    if (n32 > 0) {  // the block's FP32 list, on the next stream (beside its FP64 list)
       a.work_count = B.d_counts32 + k;
       a.reverse = 1;
       a.fp32 = 1;
       a.ticket = tickets ? tickets + 2 * k + 1 : nullptr;
       const int grid32 = (int)std::max<long long>(
           1, std::min<long long>((n32 * h.team + 127) / 128, (long long)nsm * h.ctas_per_sm));
-      if ((s = launch_class(la, lb, lc, ld, a, grid32, bs))) return s;
+      const cudaStream_t bs32 = nstreams ? B.aux[(i + 1) % nstreams] : st;
+      if ((s = launch_class(la, lb, lc, ld, a, grid32, bs32))) return s;
     }
   }
   if (per_block) cudaEventRecord(B.blk_ev[nblk], st);
@@ -1067,6 +1173,7 @@ __global__ void expand_jwork(const long long* __restrict__ row_start, int nrows,
 
 int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t st, double skip,
                 double fp32) {
+  NvtxRange range("gbx direct Coulomb matrix");
   int s;
   const bool mixed = skip > 0.0 || fp32 > 0.0;
   if (mixed && B.potential)
@@ -1195,6 +1302,7 @@ int run_coulomb(Basis& B, const double* D, double tau, double* J, cudaStream_t s
       a.work_off = 0;
       a.nwork = len;
       a.mode = 2;
+      a.fault = B.d_fault;
       a.team = h.team;
       a.variant = h.variant;
       a.fp32 = L.fp32;
@@ -1264,6 +1372,10 @@ static ExpandArgs expand_args(const Basis& B, int notation, double* out) {
   e.rowinfo = B.d_rowinfo;
   e.npf = B.pf_first[kNumPairClasses];
   for (int c = 0; c <= kNumPairClasses; ++c) e.pf_first[c] = B.pf_first[c];
+  e.fault = B.d_fault;
+  e.out_lo = out;
+  e.out_len = B.nbf * B.nbf * B.nbf * B.nbf;
+  e.compact_len = B.compact_elems;
   return e;
 }
 
@@ -1328,6 +1440,7 @@ static int ensure_pinned_ring(size_t elems, double** ring) {
 // the next ones expand.  Host memory may be pageable or page-locked (page-locked copies run
 // asynchronously and overlap fully).  Synchronous.
 int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStream_t st) {
+  NvtxRange range("gbx full tensor to host");
   const long long n = B.nbf;
   const size_t slab = (size_t)n * n * n;  // elements of one x
   const size_t row_bytes = (size_t)B.pf_first[kNumPairClasses] * sizeof(double);
@@ -1388,7 +1501,10 @@ int run_full_host(Basis& B, int notation, double tau, double* out_host, cudaStre
     if (i >= kStageBuffers) GBX_CUDA(cudaStreamWaitEvent(st, B.stage_free[k], 0), "wait slab");
     const long long planes = (x1 - x0) * n;
     const int grid = (int)std::max<long long>(1, std::min<long long>(planes, (long long)nsm * per_sm));
-    expand_slab<<<grid, 512, row_bytes, st>>>(e, x0, x1, buf);
+    ExpandArgs es = e;  // this launch's destination: the slab
+    es.out_lo = buf;
+    es.out_len = (x1 - x0) * slab;
+    expand_slab<<<grid, 512, row_bytes, st>>>(es, x0, x1, buf);
     GBX_CUDA(cudaGetLastError(), "expand_slab launch");
     GBX_CUDA(cudaEventRecord(B.stage_ready[k], st), "record slab");
     GBX_CUDA(cudaStreamWaitEvent(B.copy_stream, B.stage_ready[k], 0), "wait slab");
@@ -1453,6 +1569,7 @@ int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, d
              double fp32) {
   int s = run_compact(B, tau, st, skip, fp32);
   if (s) return s;
+  NvtxRange range("gbx expansion");
   const ExpandArgs e = expand_args(B, notation, out);
   if (B.profiling) cudaEventRecord(B.ev[2], st);
   const size_t row_bytes = (size_t)e.npf * sizeof(double);
@@ -1479,6 +1596,7 @@ int run_full(Basis& B, int notation, double tau, double* out, cudaStream_t st, d
 // J and K of a density from the unique integrals (compact store; the N^4 tensor is never
 // formed).  D, J, K: device N x N row-major.
 int run_jk(Basis& B, const double* D, double tau, double* J, double* K, cudaStream_t st) {
+  NvtxRange range("gbx J and K");
   int s = run_compact(B, tau, st, 0.0, 0.0);
   if (s) return s;
   const ExpandArgs e = expand_args(B, GBX_CHEMIST, nullptr);

@@ -24,6 +24,11 @@ struct ExpandArgs {
   const BlockDev* blocks;
   const double* compact;
   double* out;
+  // debug builds: fault word, the valid destination range [out_lo, out_lo + out_len) of the
+  // launch (the tensor or a host-copy slab) and the compact store's length
+  unsigned long long* fault;
+  const double* out_lo;
+  long long out_len, compact_len;
   const long long* ftab;  // n*n function-pair keys (class, pair index in class, block row)
   // row-staged form (expand_rows)
   const int* gtab;        // n*n: pair function (class-major index) of each ordered pair
@@ -42,6 +47,12 @@ struct MixedParams {
   double skip, fp32;
   int* counts32;
   const int* fp32_on;  // per block: 1 = FP32 list in use (nullptr: every block with an FP32 path)
+  // left-out quartets (bound below skip) listed for zero_quartets, which clears only their
+  // entries of the compact store; nullptr: they are dropped (the caller clears the store)
+  int2* zero_work;
+  int* zero_count;
+  long long zero_cap;
+  unsigned long long* fault;  // debug builds: the call's fault word (work-list indices)
 };
 
 __global__ void build_work(const int2* __restrict__ cta_map, const BuildBlock* __restrict__ bb,

@@ -121,6 +121,38 @@ struct DeviceGuard {
   }
 };
 
+// ------------------------------------------------------------ debug bounds checks
+int check_bounds_fault(unsigned long long* d_fault, cudaStream_t st, const char* what) {
+#if GBX_DEBUG_BOUNDS
+  if (!d_fault) return GBX_OK;
+  unsigned long long f = 0;
+  GBX_CUDA(cudaStreamSynchronize(st), "bounds check: synchronize");
+  GBX_CUDA(cudaMemcpy(&f, d_fault, sizeof(f), cudaMemcpyDeviceToHost), "bounds check: read");
+  if (!f) return GBX_OK;
+  GBX_CUDA(cudaMemset(d_fault, 0, sizeof(f)), "bounds check: clear");
+  static const char* const sites[] = {"?", "class-kernel store", "work-list build", "zero fill",
+                                      "expansion store", "compact-store read", "J/K scatter"};
+  const unsigned site = (unsigned)(f >> 56);
+  const unsigned long long idx = f & 0x00ffffffffffffffull;
+  return set_error(GBX_ERR_INVALID, "%s: out-of-range index %llu at the %s", what, idx,
+                   sites[site < 7 ? site : 0]);
+#else
+  (void)d_fault;
+  (void)st;
+  (void)what;
+  return GBX_OK;
+#endif
+}
+
+int alloc_fault_word(unsigned long long** d_fault) {
+  *d_fault = nullptr;
+#if GBX_DEBUG_BOUNDS
+  GBX_CUDA(cudaMalloc((void**)d_fault, sizeof(unsigned long long)), "cudaMalloc(fault word)");
+  GBX_CUDA(cudaMemset(*d_fault, 0, sizeof(unsigned long long)), "clear fault word");
+#endif
+  return GBX_OK;
+}
+
 // ------------------------------------------------------------------- block cache
 // Device blocks a basis gives back are kept for the next basis in the process, up to
 // kBlockCacheBytes per device: the public full-tensor call builds and drops a basis every time,
@@ -255,6 +287,7 @@ int Basis::ensure_out(size_t elems) {
 int build_basis(Basis& B, int n, const int* angmom, const int* nprim, const double* center,
                        const double* exps, const double* coefs, const int* nout, const int* sph,
                        const int8_t* pos, const double* scl) {
+  NvtxRange range("gbx build basis");
   B.shells.resize(n);
   int prim_total = 0, func = 0;
   for (int s = 0; s < n; ++s) {
@@ -461,12 +494,14 @@ int coulomb_entry(gbx_basis* b, const double* D, double tau, double* J, cudaStre
                   double skip, double fp32) {
   Basis& B = *b->impl;
   DeviceGuard g(B.device);
-  return run_coulomb(B, D, tau, J, st, skip, fp32);
+  const int s = run_coulomb(B, D, tau, J, st, skip, fp32);
+  return s ? s : check_bounds_fault(B.d_fault, st, "gbx_eri_coulomb_j");
 }
 int jk_entry(gbx_basis* b, const double* D, double tau, double* J, double* K, cudaStream_t st) {
   Basis& B = *b->impl;
   DeviceGuard g(B.device);
-  return run_jk(B, D, tau, J, K, st);
+  const int s = run_jk(B, D, tau, J, K, st);
+  return s ? s : check_bounds_fault(B.d_fault, st, "gbx_eri_jk");
 }
 int point_charge_entry(gbx_basis* b, int npoints, const double* coords, const double* charges,
                        int sum, double* out, cudaStream_t st) {
@@ -500,6 +535,12 @@ int gbx_release_cached_memory(void) {
     DeviceGuard g(b.device);
     cudaFree(b.p);
   }
+  return GBX_OK;
+}
+
+int gbx_debug_bounds(int* on) {
+  if (!on) return set_error(GBX_ERR_INVALID, "gbx_debug_bounds: null argument");
+  *on = GBX_DEBUG_BOUNDS ? 1 : 0;
   return GBX_OK;
 }
 
@@ -558,7 +599,8 @@ int gbx_eri_full(gbx_basis* b, int notation, double tau, double* out, void* stre
   if (!(tau >= 0.0)) return set_error(GBX_ERR_INVALID, "schwarz threshold must be >= 0");
   Basis& B = *b->impl;
   DeviceGuard g(B.device);
-  return run_full(B, notation, tau, out, (cudaStream_t)stream);
+  const int s = run_full(B, notation, tau, out, (cudaStream_t)stream);
+  return s ? s : check_bounds_fault(B.d_fault, (cudaStream_t)stream, "gbx_eri_full");
 }
 
 int gbx_eri_full_mixed(gbx_basis* b, int notation, double skip, double fp32, double* out,
@@ -570,7 +612,8 @@ int gbx_eri_full_mixed(gbx_basis* b, int notation, double skip, double fp32, dou
     return set_error(GBX_ERR_INVALID, "thresholds must be >= 0");
   Basis& B = *b->impl;
   DeviceGuard g(B.device);
-  return run_full(B, notation, 0.0, out, (cudaStream_t)stream, skip, fp32);
+  const int s = run_full(B, notation, 0.0, out, (cudaStream_t)stream, skip, fp32);
+  return s ? s : check_bounds_fault(B.d_fault, (cudaStream_t)stream, "gbx_eri_full_mixed");
 }
 
 int gbx_eri_unique(gbx_basis* b, double skip, double fp32, void* stream) {
@@ -579,7 +622,8 @@ int gbx_eri_unique(gbx_basis* b, double skip, double fp32, void* stream) {
     return set_error(GBX_ERR_INVALID, "thresholds must be >= 0");
   Basis& B = *b->impl;
   DeviceGuard g(B.device);
-  return run_compact(B, 0.0, (cudaStream_t)stream, skip, fp32);
+  const int s = run_compact(B, 0.0, (cudaStream_t)stream, skip, fp32);
+  return s ? s : check_bounds_fault(B.d_fault, (cudaStream_t)stream, "gbx_eri_unique");
 }
 
 int gbx_compact_view(gbx_basis* b, const double** dev_ptr, int64_t* n_elems) {
@@ -607,7 +651,8 @@ int gbx_eri_full_host(gbx_basis* b, int notation, double tau, double* out_host, 
   if (!(tau >= 0.0)) return set_error(GBX_ERR_INVALID, "schwarz threshold must be >= 0");
   Basis& B = *b->impl;
   DeviceGuard g(B.device);
-  return run_full_host(B, notation, tau, out_host, (cudaStream_t)stream);
+  const int s = run_full_host(B, notation, tau, out_host, (cudaStream_t)stream);
+  return s ? s : check_bounds_fault(B.d_fault, (cudaStream_t)stream, "gbx_eri_full_host");
 }
 
 int gbx_schwarz_bounds(gbx_basis* b, double* q_host) {
@@ -744,15 +789,48 @@ int gbx_last_counts(const gbx_basis* b, int64_t* computed, int64_t* screened) {
     if (screened) *screened = B.last_screened;
     return GBX_OK;
   }
+  int64_t n64 = 0, n32 = 0, nleft = 0;
+  int s = gbx_mixed_counts(b, &n64, &n32, &nleft);
+  if (s) return s;
+  if (computed) *computed = n64 + n32;
+  if (screened) *screened = B.n_quartets - n64 - n32;
+  return GBX_OK;
+}
+
+int gbx_basis_set_fp32_lists(gbx_basis* b, int64_t min_quartets, int64_t share) {
+  if (!b || min_quartets < 0 || share < 1)
+    return set_error(GBX_ERR_INVALID, "gbx_basis_set_fp32_lists: need min >= 0 and share >= 1");
+  Basis& B = *b->impl;
+  B.fp32_min = min_quartets;
+  B.fp32_share = share;
+  B.mix_n32.clear();  // recount the lists at the next mixed call
+  return GBX_OK;
+}
+
+int gbx_mixed_counts(const gbx_basis* b, int64_t* n_fp64, int64_t* n_fp32, int64_t* n_left_out) {
+  if (!b) return set_error(GBX_ERR_INVALID, "gbx_mixed_counts: null basis");
+  Basis& B = *b->impl;
+  if (n_fp64) *n_fp64 = 0;
+  if (n_fp32) *n_fp32 = 0;
+  if (n_left_out) *n_left_out = 0;
+  if (!B.d_counts) return GBX_OK;  // no compact-store call yet
   DeviceGuard g(B.device);
   const int nblk = (int)B.blocks.size();
-  std::vector<int> c(nblk);
+  std::vector<int> c(nblk), c32(nblk, 0);
   GBX_CUDA(cudaMemcpy(c.data(), B.d_counts, nblk * sizeof(int), cudaMemcpyDeviceToHost),
            "read quartet counters");
-  long long tot = 0;
-  for (int v : c) tot += v;
-  if (computed) *computed = tot;
-  if (screened) *screened = B.n_quartets - tot;
+  if (B.last_mixed && B.d_counts32)
+    GBX_CUDA(cudaMemcpy(c32.data(), B.d_counts32, nblk * sizeof(int), cudaMemcpyDeviceToHost),
+             "read FP32 quartet counters");
+  long long t64 = 0, t32 = 0;
+  for (int k = 0; k < nblk; ++k) {
+    t64 += c[k];
+    t32 += c32[k];
+  }
+  if (n_fp64) *n_fp64 = t64;
+  if (n_fp32) *n_fp32 = t32;
+  // left out: every quartet not computed (the mixed form's skip, or a Schwarz threshold)
+  if (n_left_out) *n_left_out = B.n_quartets - t64 - t32;
   return GBX_OK;
 }
 

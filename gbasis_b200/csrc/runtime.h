@@ -1,6 +1,7 @@
 // Host-side state of a basis handle (internal to libgbx_eri).
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <utility>
 #include <vector>
@@ -11,9 +12,25 @@
 
 namespace gbx {
 
+// Named host-phase range for timeline profilers (NVTX push/pop; without an attached tool the
+// calls return at once).  Entry points and their phases (basis upload, Schwarz bounds, work
+// list and class kernels, expansion, host copies) open one for their scope.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 constexpr int kAuxStreams = 6;      // default concurrent class-block streams of a basis
 constexpr int kMaxAuxStreams = 16;  // the most a basis may be given
-constexpr long long kMinFp32List = 2048;  // mixed form: smallest FP32 list given its own launch
+// mixed form: smallest FP32 list given its own launch, and its least share of the block (1 in
+// kFp32ListShare).  A list below either stays in the FP64 list: measured on the 120-function
+// full tensor, lists of 2,048 quartets and a twentieth of a block (20,524 quartets in all)
+// made the call 4 % slower than FP64 (their launches, Boys-table staging and tails cost more
+// than FP32 recursions save on classes whose time goes to the Boys function)
+constexpr long long kMinFp32List = 65536;
+constexpr long long kFp32ListShare = 4;
 constexpr long long kCoulombChunk = 1LL << 23;  // quartets per direct-Coulomb work chunk
 constexpr int kStageBuffers = 3;                // host-output staging slabs in flight
 constexpr size_t kStageBytes = 64ull << 20;     // target bytes of one staging slab
@@ -103,7 +120,13 @@ struct Basis {
   // mixed form: per block, upper bounds of the FP32 and left-out quartets at (skip, fp32)
   std::vector<long long> mix_n32, mix_nskip;
   double mix_key_skip = -1.0, mix_key_fp32 = -1.0;
-  int* d_fp32_on = nullptr;  // per block: FP32 list in use  // the last call counted its quartets on the host (direct J)
+  int* d_fp32_on = nullptr;  // per block: FP32 list in use
+  int2* d_zero_work = nullptr;  // mixed form: left-out quartets of a call (zero_quartets)
+  int* d_zero_count = nullptr;
+  long long zero_cap = 0;
+  bool last_mixed = false;  // the last compact-store call ran the mixed form
+  long long fp32_min = kMinFp32List, fp32_share = kFp32ListShare;  // FP32 list rule
+  unsigned long long* d_fault = nullptr;  // debug builds: fault word of the bounds checks
   // optional phase timing with events on the launching stream:
   // [0] work-list build, [1] class kernels, [2] expansion
   bool profiling = false;
@@ -149,6 +172,12 @@ int run_jk(Basis& B, const double* D, double tau, double* J, double* K, cudaStre
 int run_point_charge(Basis& B, int npoints, const double* coords, const double* charges,
                      int sum, double* out, cudaStream_t st);
 int ensure_schwarz(Basis& B, cudaStream_t st);
+// Debug builds (GBX_DEBUG_BOUNDS): waits for the call's work on `st` and returns
+// GBX_ERR_INVALID naming the site and index of the first out-of-range access recorded in
+// *d_fault (then cleared); release builds return GBX_OK at once.
+int check_bounds_fault(unsigned long long* d_fault, cudaStream_t st, const char* what);
+// Debug builds: a cleared fault word on the device (nullptr in release builds).
+int alloc_fault_word(unsigned long long** d_fault);
 int unique_values(Basis& B, long long n, const long long* idx4_host, double* out_host,
                   cudaStream_t st);
 struct ExpandArgs;

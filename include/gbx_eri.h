@@ -174,6 +174,13 @@ int gbx_batch_info(const gbx_batch* b, int64_t* nbf, int64_t* n_quartets,
 int gbx_batch_run(gbx_batch* b, int notation, double* const* outs, void* stream);
 /* 1 (default): replay a captured CUDA graph; 0: launch eagerly every run. */
 int gbx_batch_set_graph(gbx_batch* b, int on);
+/* 1: the FP64 run's class kernels become ONE persistent launch (a multi-class work queue:
+ * every block type's quartets, largest types first, drawn by warps from a single counter and
+ * evaluated by the class's recursion programs), followed by the batched expansion, captured
+ * and replayed as above; 0 (default): one class kernel per block type.  The mixed form and
+ * per-type profiling always use the per-type kernels.  Changing it drops the captured graph.
+ * No counterpart in the reference (a Python loop of per-molecule calls). */
+int gbx_batch_set_queue(gbx_batch* b, int on);
 /* Block types of a batch (one class kernel launch each) and their team of lanes per quartet
  * (register kernel; the autotuner's knob).  Setting a team drops the captured graph.  With
  * profiling on, runs launch the types one after another (no graph) and gbx_batch_type_times
@@ -225,6 +232,18 @@ int gbx_eri_jk(gbx_basis* b, const double* D, double schwarz_threshold, double* 
 /* Device-side counters of the last call on this basis: quartets computed and screened. */
 int gbx_last_counts(const gbx_basis* b, int64_t* computed, int64_t* screened);
 
+/* Quartets of the last compact-store call on this basis (full tensor or unique integrals) by
+ * treatment: computed in FP64, computed with FP32 recursions (mixed form), and left out (their
+ * integrals are zero: below the mixed form's skip bound, or screened).  No counterpart in the
+ * reference: gbasis computes every quartet in FP64. */
+int gbx_mixed_counts(const gbx_basis* b, int64_t* n_fp64, int64_t* n_fp32, int64_t* n_left_out);
+
+/* Mixed form: a class block's FP32 quartets get their own FP32 launch only when they number at
+ * least min_quartets and at least 1/share of the block; otherwise they stay in its FP64 list
+ * (default 65536 and 4: smaller lists cost more in launch, table staging and tail than FP32
+ * saves).  No counterpart in the reference. */
+int gbx_basis_set_fp32_lists(gbx_basis* b, int64_t min_quartets, int64_t share);
+
 /* Phase timing: level 1 records CUDA events on the call's stream around the work-list
  * build, the class kernels and the expansion (gbx_phase_times waits for the last call and
  * returns the three durations in ms); level 2 also times every class block, running them
@@ -269,6 +288,14 @@ int gbx_release_cached_memory(void);
 
 /* Copy of the last error message on this thread (NUL-terminated, truncated to len). */
 int gbx_last_error(char* buf, size_t len);
+
+/* *on = 1 in the bounds-checking build (libgbx_eri_debug.so, compiled with
+ * GBX_DEBUG_BOUNDS=1), else 0.  In that build every kernel store into the compact store, the
+ * work lists, the N^4 tensor (or a host-copy slab) and J / K, and every compact-store read
+ * of the expansions, is index-checked; a call whose kernels went out of range waits for its
+ * stream and returns GBX_ERR_INVALID naming the site and the index, instead of writing there.
+ * It stands in for a device memory checker.  No counterpart in the reference. */
+int gbx_debug_bounds(int* on);
 
 /* Sustained FP64 FMA rate of the device (TFLOP/s) from a dependent-FMA microbenchmark. */
 int gbx_fp64_peak(int device, double* tflops);

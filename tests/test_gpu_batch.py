@@ -214,12 +214,18 @@ def test_batch_heavily_contracted_quartets_against_oracle():
     b = EriBatch(mols)
     outs = [torch.empty((n,) * 4, dtype=torch.float64, device="cuda") for n in b.nbf]
     b.run(outs)
+    # the multi-class queue form of the same batch (recursion programs of each class)
+    b.set_queue(True)
+    outs_q = [torch.empty_like(t) for t in outs]
+    b.run(outs_q)
     torch.cuda.synchronize()
     rng = np.random.default_rng(11)
     procs = min(os.cpu_count() or 1, 32)
     beyond = checked = 0
-    for m, shells, out in zip(big, mols, outs):
+    q_worst = q_ratio = 0.0
+    for m, shells, out, out_q in zip(big, mols, outs, outs_q):
         T = out.cpu().numpy()
+        TQ = out_q.cpu().numpy()
         nf = np.array([len(s.angmom_components_cart) for s in shells])
         off = np.concatenate([[0], np.cumsum(nf)])
         pairs = opar.unique_pairs(len(shells))
@@ -244,6 +250,73 @@ def test_batch_heavily_contracted_quartets_against_oracle():
             assert err <= max(1e-9, 4.0 * ref_err), (m, (i, j, kk, ll), err, ref_err)
             beyond += err > max(1e-11, 4.0 * ref_err)
             checked += 1
+            bq = TQ[off[i]:off[i + 1], off[j]:off[j + 1], off[kk]:off[kk + 1], off[ll]:off[ll + 1]]
+            err_q = float(np.abs(bq - t).max())
+            q_worst = max(q_worst, err_q)
+            q_ratio = max(q_ratio, err_q / max(ref_err, 1e-300))
+            # queue form: within the reference's own error scale on these quartets
+            assert err_q <= max(5e-8, 4.0 * ref_err), (m, (i, j, kk, ll), err_q, ref_err)
         assert pos == truth.size
+    print(f"queue form: largest error {q_worst:.3e}, largest error / reference's {q_ratio:.3e}")
     assert beyond * 20 <= checked, (beyond, checked)
     b.close()
+
+
+def test_batch_queue_form_against_oracle_and_per_type_kernels():
+    """The multi-class queue form (one persistent launch draining every block type's quartets
+    from a single counter): small molecules against the oracle at the FP64 bar; 24 batch
+    molecules against the per-type kernels (other recursion code: within 1e-9, the engine's
+    own error bound on the batch's heavily contracted quartets, with most elements at 1e-12);
+    graph replays bit for bit."""
+    import torch
+    small = [make_workload("tiny4")] + [m for m in (batch_molecule(k) for k in range(200))
+                                        if sum(len(s.angmom_components_cart) for s in m) <= 24][:3]
+    q = EriBatch(small)
+    q.set_queue(True)
+    outs = [torch.empty((n,) * 4, dtype=torch.float64, device="cuda") for n in q.nbf]
+    q.run(outs)
+    torch.cuda.synchronize()
+    for shells, t in zip(small, outs):
+        ref = orc.electron_repulsion_integral(shells, notation="chemist", reorder="exponent")
+        np.testing.assert_allclose(t.cpu().numpy(), ref, rtol=0, atol=ATOL)
+    q.close()
+
+    mols = [batch_molecule(m) for m in range(24)]
+    per_type = EriBatch(mols)
+    queue = EriBatch(mols)
+    queue.set_queue(True)
+    ref = [torch.empty((n,) * 4, dtype=torch.float64, device="cuda") for n in per_type.nbf]
+    got = [torch.full((n,) * 4, np.nan, dtype=torch.float64, device="cuda") for n in queue.nbf]
+    per_type.run(ref)
+    queue.run(got)  # captures the queue graph
+    torch.cuda.synchronize()
+    worst, beyond, total = 0.0, 0, 0
+    for shells, a, b in zip(mols, got, ref):
+        d = (a - b).abs()
+        if float(d.max()) > worst:
+            worst = float(d.max())
+            # shells (angular momentum, primitives) of the largest difference
+            idx = np.unravel_index(int(d.argmax()), tuple(d.shape))
+            owner = np.repeat(np.arange(len(shells)),
+                              [len(sh.angmom_components_cart) for sh in shells])
+            where = [(shells[owner[i]].angmom, len(shells[owner[i]].exps)) for i in idx]
+        beyond += int((d > ATOL).sum())
+        total += d.numel()
+    print(f"largest difference at shells (l, K) {where}")
+    print(f"queue vs per-type kernels: max |diff| {worst:.3e}, {beyond} of {total} beyond {ATOL}")
+    # the two recursion codes differ only on heavily contracted quartets, where contracted
+    # recursions lose digits (checked against exact values in the heavily contracted test)
+    assert worst <= 1e-7
+    assert beyond * 1000 <= total
+    again = [torch.empty_like(t) for t in got]
+    queue.run(again)  # replay
+    torch.cuda.synchronize()
+    for a, b in zip(got, again):
+        assert torch.equal(a, b)
+    queue.set_queue(False)  # back to the per-type kernels: same values as the other batch
+    queue.run(again)
+    torch.cuda.synchronize()
+    for a, b in zip(again, ref):
+        assert torch.equal(a, b)
+    per_type.close()
+    queue.close()

@@ -39,3 +39,34 @@ def test_mixed_error_below_1e10(name):
     rel = (err[big] / np.abs(ref[big])).max() if big.any() else 0.0
     print(f"{name}: N={ref.shape[0]} max abs {err.max():.3e} max rel (|ref|>1e-8) {rel:.3e}")
     assert err.max() <= 1e-10
+
+
+def test_left_out_quartets_zeroed_in_a_dirty_store():
+    """The mixed form writes zeros for its left-out quartets itself (no clearing of the whole
+    compact store): with every store entry set to NaN before the call, the expanded tensor has
+    no NaN, matches the FP64 tensor at the mixed bar, and the quartet counts add up."""
+    import torch
+    from gbasis_b200 import _engine
+    from gbasis_b200.electron_repulsion import MIXED_FP32, MIXED_SKIP
+    shells = make_workload("large64")[:40]  # 4 atoms of the 20-bohr box: many left out
+    db = _engine.DeviceBasis(shells)
+    n = db.nbf
+    ref = torch.empty(n ** 4, dtype=torch.float64, device="cuda")
+    db.full_device(ref.data_ptr())
+    torch.cuda.synchronize()
+    n64_ref, n32_ref, left_ref = db.mixed_counts()
+    assert n32_ref == 0 and left_ref == 0 and n64_ref == db.stats()[0]
+    got = torch.empty_like(ref)
+    db.set_fp32_lists(1, 1 << 30)  # every block's FP32 quartets get their own launch here
+    for _ in range(2):  # the second call reuses the zero list
+        db.compact_view().fill_(float("nan"))
+        got.fill_(float("nan"))
+        db.full_device(got.data_ptr(), mixed=(MIXED_SKIP, MIXED_FP32))
+        torch.cuda.synchronize()
+        n64, n32, left = db.mixed_counts()
+        print(f"N={n}: quartets FP64 {n64} FP32 {n32} left out {left}")
+        assert left > 0 and n32 > 0
+        assert n64 + n32 + left == db.stats()[0]
+        assert not torch.isnan(got).any()
+        assert float((got - ref).abs().max()) <= 1e-10
+    db.close()
