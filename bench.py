@@ -258,7 +258,8 @@ def run_reference(a, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def extra_configs(local, reps=2, large_atoms=16):
+def extra_configs(local, reps=2, large_atoms=16,
+                  which=("chain20", "batch512", "large64")):
     """The other configurations of the path, each timed on the device with CUDA events on the
     launching stream (one warm-up call, then ``reps`` calls):
 
@@ -298,153 +299,156 @@ def extra_configs(local, reps=2, large_atoms=16):
         return e0.elapsed_time(e1) / n
 
     out = {}
-    shells = make_workload("chain20")
-    db = _engine.DeviceBasis(shells, device=local)
-    uq, fl = unique_eris(db.nbf), basis_flops(shells)
-    ms64 = timed(lambda: db.unique(stream=sp))
-    ref = db.compact_view().clone()
-    msmx = timed(lambda: db.unique((MIXED_SKIP, MIXED_FP32), stream=sp))
-    cur = db.compact_view()
-    max_abs = max_rel = 0.0
-    for c0 in range(0, ref.numel(), 1 << 27):
-        r, x = ref[c0:c0 + (1 << 27)], cur[c0:c0 + (1 << 27)]
-        d = (x - r).abs()
-        max_abs = max(max_abs, float(d.max()))
-        max_rel = max(max_rel, float((d / r.abs().clamp_min(1e-8)).max()))
-    out["chain20_unique"] = {
-        "n_functions": db.nbf, "unique_eris": uq, "shell_quartets": db.stats()[0],
-        "fp64": {"ms": ms64, "value": uq / (ms64 * 1e-3), "unit": UNIT,
-                 "achieved_tflops": fl / (ms64 * 1e-3) / 1e12, "frac_fp64_peak": fl / (ms64 * 1e-3) / 1e12 / peak64},
-        "mixed": {"ms": msmx, "value": uq / (msmx * 1e-3), "unit": UNIT, "speedup_vs_fp64": ms64 / msmx,
-                  "max_abs_err_vs_fp64": max_abs, "max_rel_err_vs_fp64": max_rel,
-                  "error_over": "every unique integral", "skip_bound": MIXED_SKIP,
-                  "fp32_bound": MIXED_FP32}}
-    del ref, cur, r, x, d
-    try:  # the oracle's Cartesian blocks on a sample of this workload's quartets, 1 core
-        out["chain20_unique"]["cpu_baseline"] = cpu_baseline(shells, seconds=8.0, seed=3,
-                                                             n_functions=db.nbf)
-    except Exception as exc:
-        out["chain20_unique"]["cpu_baseline"] = {"error": str(exc)[:300]}
-    db.close()
-    torch.cuda.empty_cache()
+    if "chain20" in which:
+        shells = make_workload("chain20")
+        db = _engine.DeviceBasis(shells, device=local)
+        uq, fl = unique_eris(db.nbf), basis_flops(shells)
+        ms64 = timed(lambda: db.unique(stream=sp))
+        ref = db.compact_view().clone()
+        msmx = timed(lambda: db.unique((MIXED_SKIP, MIXED_FP32), stream=sp))
+        cur = db.compact_view()
+        max_abs = max_rel = 0.0
+        for c0 in range(0, ref.numel(), 1 << 27):
+            r, x = ref[c0:c0 + (1 << 27)], cur[c0:c0 + (1 << 27)]
+            d = (x - r).abs()
+            max_abs = max(max_abs, float(d.max()))
+            max_rel = max(max_rel, float((d / r.abs().clamp_min(1e-8)).max()))
+        out["chain20_unique"] = {
+            "n_functions": db.nbf, "unique_eris": uq, "shell_quartets": db.stats()[0],
+            "fp64": {"ms": ms64, "value": uq / (ms64 * 1e-3), "unit": UNIT,
+                     "achieved_tflops": fl / (ms64 * 1e-3) / 1e12, "frac_fp64_peak": fl / (ms64 * 1e-3) / 1e12 / peak64},
+            "mixed": {"ms": msmx, "value": uq / (msmx * 1e-3), "unit": UNIT, "speedup_vs_fp64": ms64 / msmx,
+                      "max_abs_err_vs_fp64": max_abs, "max_rel_err_vs_fp64": max_rel,
+                      "error_over": "every unique integral", "skip_bound": MIXED_SKIP,
+                      "fp32_bound": MIXED_FP32}}
+        del ref, cur, r, x, d
+        try:  # the oracle's Cartesian blocks on a sample of this workload's quartets, 1 core
+            out["chain20_unique"]["cpu_baseline"] = cpu_baseline(shells, seconds=8.0, seed=3,
+                                                                 n_functions=db.nbf)
+        except Exception as exc:
+            out["chain20_unique"]["cpu_baseline"] = {"error": str(exc)[:300]}
+        db.close()
+        torch.cuda.empty_cache()
 
-    mols = make_workload("batch512")
-    t0 = time.perf_counter()
-    b = EriBatch(mols, device=local)
-    t_create = time.perf_counter() - t0
-    outs = [torch.empty((n,) * 4, dtype=torch.float64, device=dev) for n in b.nbf]
-    ms = timed(lambda: b.run(outs, stream=sp))
-    uq = sum(unique_eris(n) for n in b.nbf)
-    fl = sum(basis_flops(m) for m in mols)
-    out["batch512"] = {
-        "molecules": len(mols), "unique_eris": uq, "shell_quartets": b.n_quartets,
-        "tensor_bytes": 8 * sum(n ** 4 for n in b.nbf), "ms": ms,
-        "value": uq / (ms * 1e-3), "unit": UNIT, "molecules_per_s": len(mols) / (ms * 1e-3),
-        "achieved_tflops": fl / (ms * 1e-3) / 1e12, "frac_fp64_peak": fl / (ms * 1e-3) / 1e12 / peak64,
-        "create_s": t_create, "launch": "one CUDA graph replay per run"}
-    try:  # the same block types one after another with events between them (no overlap)
-        Lb = _engine.lib()
-        _engine.check(Lb.gbx_batch_set_profiling(b.handle, 1))
-        b.run(outs, stream=sp)
-        torch.cuda.synchronize()
-        tms = np.zeros(len(b.types()))
-        _engine.check(Lb.gbx_batch_type_times(b.handle, tms.ctypes.data_as(ctypes.c_void_p), len(tms)))
-        _engine.check(Lb.gbx_batch_set_profiling(b.handle, 0))
-        out["batch512"]["types_serial_ms"] = float(tms.sum())
-        out["batch512"]["heavy_types_serial_ms"] = float(sum(
-            t for (c4, _, _, _), t in zip(b.types(), tms) if not light_class(c4)))
-    except Exception as exc:
-        out["batch512"]["types_serial_ms"] = {"error": str(exc)[:200]}
-    # mixed form of the same batch, side by side (its own graph); error against the FP64
-    # tensors of every 8th molecule with N <= 80
-    try:
-        th = (MIXED_SKIP, MIXED_FP32)
-        sample = [m for m in range(0, len(mols), 8) if b.nbf[m] <= 80]
-        ref = {m: outs[m].clone() for m in sample}
+    if "batch512" in which:
+        mols = make_workload("batch512")
         t0 = time.perf_counter()
-        b.run(outs, stream=sp, mixed=th)  # first mixed run: bounds and lists
-        torch.cuda.synchronize()
-        t_setup = time.perf_counter() - t0
-        ms_mx = timed(lambda: b.run(outs, stream=sp, mixed=th))
-        err = max(float((outs[m] - ref[m]).abs().max()) for m in sample)
-        n64, n32, nskip = b.mixed_counts()
-        out["batch512"]["mixed"] = {
-            "ms": ms_mx, "value": uq / (ms_mx * 1e-3), "unit": UNIT,
-            "speedup_vs_fp64": ms / ms_mx, "max_abs_err_vs_fp64": err,
-            "error_over": f"full tensors of {len(sample)} molecules (every 8th with N <= 80)",
-            "quartets_fp64": n64, "quartets_fp32": n32, "quartets_left_out": nskip,
-            "first_run_s": t_setup, "skip_bound": MIXED_SKIP, "fp32_bound": MIXED_FP32}
-        del ref
-    except Exception as exc:  # keep the rest of the line
-        out["batch512"]["mixed"] = {"error": str(exc)[:300]}
-    # the multi-class queue form: one persistent launch for every block type (then the
-    # batched expansion), captured and replayed like the per-type graph; its largest
-    # difference from the per-type kernels' tensors over the same sampled molecules
-    try:
-        sample = [m for m in range(0, len(mols), 8) if b.nbf[m] <= 80]
-        b.run(outs, stream=sp)
-        torch.cuda.synchronize()
-        ref = {m: outs[m].clone() for m in sample}
-        b.set_queue(True)
-        ms_q = timed(lambda: b.run(outs, stream=sp))
-        diff = max(float((outs[m] - ref[m]).abs().max()) for m in sample)
-        b.set_queue(False)
-        out["batch512"]["queue"] = {
-            "ms": ms_q, "value": uq / (ms_q * 1e-3), "unit": UNIT,
-            "speedup_vs_per_type_graph": ms / ms_q, "max_abs_diff_vs_per_type": diff,
-            "launch": "one persistent multi-class queue kernel + expansion, one graph replay",
-            "default": "per-type graph" if ms <= ms_q else "queue"}
-        del ref
-    except Exception as exc:
-        out["batch512"]["queue"] = {"error": str(exc)[:300]}
-    b.close()
-    del outs
-    torch.cuda.empty_cache()
+        b = EriBatch(mols, device=local)
+        t_create = time.perf_counter() - t0
+        outs = [torch.empty((n,) * 4, dtype=torch.float64, device=dev) for n in b.nbf]
+        ms = timed(lambda: b.run(outs, stream=sp))
+        uq = sum(unique_eris(n) for n in b.nbf)
+        fl = sum(basis_flops(m) for m in mols)
+        out["batch512"] = {
+            "molecules": len(mols), "unique_eris": uq, "shell_quartets": b.n_quartets,
+            "tensor_bytes": 8 * sum(n ** 4 for n in b.nbf), "ms": ms,
+            "value": uq / (ms * 1e-3), "unit": UNIT, "molecules_per_s": len(mols) / (ms * 1e-3),
+            "achieved_tflops": fl / (ms * 1e-3) / 1e12, "frac_fp64_peak": fl / (ms * 1e-3) / 1e12 / peak64,
+            "create_s": t_create, "launch": "one CUDA graph replay per run"}
+        try:  # the same block types one after another with events between them (no overlap)
+            Lb = _engine.lib()
+            _engine.check(Lb.gbx_batch_set_profiling(b.handle, 1))
+            b.run(outs, stream=sp)
+            torch.cuda.synchronize()
+            tms = np.zeros(len(b.types()))
+            _engine.check(Lb.gbx_batch_type_times(b.handle, tms.ctypes.data_as(ctypes.c_void_p), len(tms)))
+            _engine.check(Lb.gbx_batch_set_profiling(b.handle, 0))
+            out["batch512"]["types_serial_ms"] = float(tms.sum())
+            out["batch512"]["heavy_types_serial_ms"] = float(sum(
+                t for (c4, _, _, _), t in zip(b.types(), tms) if not light_class(c4)))
+        except Exception as exc:
+            out["batch512"]["types_serial_ms"] = {"error": str(exc)[:200]}
+        # mixed form of the same batch, side by side (its own graph); error against the FP64
+        # tensors of every 8th molecule with N <= 80
+        try:
+            th = (MIXED_SKIP, MIXED_FP32)
+            sample = [m for m in range(0, len(mols), 8) if b.nbf[m] <= 80]
+            ref = {m: outs[m].clone() for m in sample}
+            t0 = time.perf_counter()
+            b.run(outs, stream=sp, mixed=th)  # first mixed run: bounds and lists
+            torch.cuda.synchronize()
+            t_setup = time.perf_counter() - t0
+            ms_mx = timed(lambda: b.run(outs, stream=sp, mixed=th))
+            err = max(float((outs[m] - ref[m]).abs().max()) for m in sample)
+            n64, n32, nskip = b.mixed_counts()
+            out["batch512"]["mixed"] = {
+                "ms": ms_mx, "value": uq / (ms_mx * 1e-3), "unit": UNIT,
+                "speedup_vs_fp64": ms / ms_mx, "max_abs_err_vs_fp64": err,
+                "error_over": f"full tensors of {len(sample)} molecules (every 8th with N <= 80)",
+                "quartets_fp64": n64, "quartets_fp32": n32, "quartets_left_out": nskip,
+                "first_run_s": t_setup, "skip_bound": MIXED_SKIP, "fp32_bound": MIXED_FP32}
+            del ref
+        except Exception as exc:  # keep the rest of the line
+            out["batch512"]["mixed"] = {"error": str(exc)[:300]}
+        # the multi-class queue form: one persistent launch for every block type (then the
+        # batched expansion), captured and replayed like the per-type graph; its largest
+        # difference from the per-type kernels' tensors over the same sampled molecules
+        try:
+            sample = [m for m in range(0, len(mols), 8) if b.nbf[m] <= 80]
+            b.run(outs, stream=sp)
+            torch.cuda.synchronize()
+            ref = {m: outs[m].clone() for m in sample}
+            b.set_queue(True)
+            ms_q = timed(lambda: b.run(outs, stream=sp))
+            diff = max(float((outs[m] - ref[m]).abs().max()) for m in sample)
+            b.set_queue(False)
+            out["batch512"]["queue"] = {
+                "ms": ms_q, "value": uq / (ms_q * 1e-3), "unit": UNIT,
+                "speedup_vs_per_type_graph": ms / ms_q, "max_abs_diff_vs_per_type": diff,
+                "launch": "one persistent multi-class queue kernel + expansion, one graph replay",
+                "default": "per-type graph" if ms <= ms_q else "queue"}
+            del ref
+        except Exception as exc:
+            out["batch512"]["queue"] = {"error": str(exc)[:300]}
+        b.close()
+        del outs
+        torch.cuda.empty_cache()
 
-    # config 5: the 64-atom box (its first `large_atoms` atoms unless 64), direct J only (the
-    # unique integrals of the whole box would take 13.6 TB)
-    shells = make_workload("large64")[: 10 * large_atoms]
-    t0 = time.perf_counter()
-    db = _engine.DeviceBasis(shells, device=local)
-    t_create = time.perf_counter() - t0
-    n = db.nbf
-    D = torch.from_numpy(density_matrix(n)).to(dev)
-    J = torch.empty((n, n), dtype=torch.float64, device=dev)
-    Jm = torch.empty((n, n), dtype=torch.float64, device=dev)
-    L = _engine.lib()
-    tau = 1e-12
+    if "large64" in which:
+        # config 5: the 64-atom box (its first `large_atoms` atoms unless 64), direct J only (the
+        # unique integrals of the whole box would take 13.6 TB)
+        shells = make_workload("large64")[: 10 * large_atoms]
+        t0 = time.perf_counter()
+        db = _engine.DeviceBasis(shells, device=local)
+        t_create = time.perf_counter() - t0
+        n = db.nbf
+        D = torch.from_numpy(density_matrix(n)).to(dev)
+        J = torch.empty((n, n), dtype=torch.float64, device=dev)
+        Jm = torch.empty((n, n), dtype=torch.float64, device=dev)
+        L = _engine.lib()
+        tau = 1e-12
 
-    def coulomb():
-        _engine.check(L.gbx_eri_coulomb_j(db.handle, ctypes.c_void_p(D.data_ptr()), tau,
-                                          ctypes.c_void_p(J.data_ptr()), sp), "gbx_eri_coulomb_j")
+        def coulomb():
+            _engine.check(L.gbx_eri_coulomb_j(db.handle, ctypes.c_void_p(D.data_ptr()), tau,
+                                              ctypes.c_void_p(J.data_ptr()), sp), "gbx_eri_coulomb_j")
 
-    def coulomb_mixed():
-        _engine.check(L.gbx_eri_coulomb_j_mixed(
-            db.handle, ctypes.c_void_p(D.data_ptr()), MIXED_SKIP, MIXED_FP32,
-            ctypes.c_void_p(Jm.data_ptr()), sp), "gbx_eri_coulomb_j_mixed")
-    # the whole box (minutes per call) is timed on its first call: that call also computes the
-    # Schwarz bounds and allocates the work buffers, well under a second of it
-    warm = large_atoms <= 16
-    ms = timed(coulomb, 1, warm)
-    computed, screened = db.last_counts()
-    ms_mx = timed(coulomb_mixed, 1, warm)
-    computed_mx, skipped_mx = db.last_counts()
-    dj = float((Jm - J).abs().max())
-    out["large64_coulomb"] = {
-        "atoms": large_atoms, "shells": len(shells), "n_functions": n, "coord_type": "spherical",
-        "candidate_quartets": computed + screened, "schwarz_threshold": tau,
-        "fp64": {"ms": ms, "quartets_computed": computed,
-                 "screened_fraction": screened / max(1, computed + screened),
-                 "quartets_per_s": computed / (ms * 1e-3),
-                 "unit": "screened unique shell quartets/s"},
-        "mixed": {"ms": ms_mx, "quartets_computed": computed_mx,
-                  "quartets_per_s": computed_mx / (ms_mx * 1e-3), "speedup_vs_fp64": ms / ms_mx,
-                  "max_abs_J_err_vs_fp64": dj, "max_abs_J": float(J.abs().max()),
-                  "skip_bound": MIXED_SKIP, "fp32_bound": MIXED_FP32},
-        "density": "D = X X^T / ||X X^T||, X seeded normal N x N/4", "create_s": t_create,
-        "warm_up_call": warm}
-    db.close()
-    torch.cuda.empty_cache()
+        def coulomb_mixed():
+            _engine.check(L.gbx_eri_coulomb_j_mixed(
+                db.handle, ctypes.c_void_p(D.data_ptr()), MIXED_SKIP, MIXED_FP32,
+                ctypes.c_void_p(Jm.data_ptr()), sp), "gbx_eri_coulomb_j_mixed")
+        # the whole box (minutes per call) is timed on its first call: that call also computes the
+        # Schwarz bounds and allocates the work buffers, well under a second of it
+        warm = large_atoms <= 16
+        ms = timed(coulomb, 1, warm)
+        computed, screened = db.last_counts()
+        ms_mx = timed(coulomb_mixed, 1, warm)
+        computed_mx, skipped_mx = db.last_counts()
+        dj = float((Jm - J).abs().max())
+        out["large64_coulomb"] = {
+            "atoms": large_atoms, "shells": len(shells), "n_functions": n, "coord_type": "spherical",
+            "candidate_quartets": computed + screened, "schwarz_threshold": tau,
+            "fp64": {"ms": ms, "quartets_computed": computed,
+                     "screened_fraction": screened / max(1, computed + screened),
+                     "quartets_per_s": computed / (ms * 1e-3),
+                     "unit": "screened unique shell quartets/s"},
+            "mixed": {"ms": ms_mx, "quartets_computed": computed_mx,
+                      "quartets_per_s": computed_mx / (ms_mx * 1e-3), "speedup_vs_fp64": ms / ms_mx,
+                      "max_abs_J_err_vs_fp64": dj, "max_abs_J": float(J.abs().max()),
+                      "skip_bound": MIXED_SKIP, "fp32_bound": MIXED_FP32},
+            "density": "D = X X^T / ||X X^T||, X seeded normal N x N/4", "create_s": t_create,
+            "warm_up_call": warm}
+        db.close()
+        torch.cuda.empty_cache()
     return out
 
 
@@ -458,6 +462,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-extra-configs", action="store_true",
                     help="skip the chain20 / batch512 / large64 measurements")
+    ap.add_argument("--configs", default="chain20,batch512,large64",
+                    help="which secondary configurations to measure (comma-separated)")
     ap.add_argument("--large64-atoms", type=int, default=16,
                     help="atoms of the 64-atom box in the direct-J configuration (64: the whole "
                          "box, about 20 minutes on one B200)")
@@ -636,7 +642,8 @@ def main():
         del out
         torch.cuda.empty_cache()
         try:  # the secondary configurations never cost the headline line
-            line["configs"] = extra_configs(local, large_atoms=a.large64_atoms)
+            line["configs"] = extra_configs(local, large_atoms=a.large64_atoms,
+                                           which=tuple(a.configs.split(",")))
         except Exception as exc:
             line["configs"] = {"error": str(exc)[:300]}
     if rank == 0 and not a.no_cpu_baseline:

@@ -20,6 +20,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import _engine
+from .base_four_symm import BaseFourIndexSymmetric, register_with_gbasis
 from .contractions import is_shell
 
 __all__ = ["ElectronRepulsionIntegral", "ElectronRepulsionIntegralImproved",
@@ -35,19 +36,6 @@ def _boys_host(orders, weighted_dist, rho=None):
     return hyp1f1(orders + 0.5, orders + 1.5, -np.asarray(weighted_dist)) / (2 * orders + 1)
 
 
-def _check_contractions(contractions):
-    # gbasis/base.py:32-65
-    if not isinstance(contractions, (list, tuple)):
-        raise TypeError("Contractions must be given as a list or tuple of "
-                        "`GeneralizedContractionShell` instance")
-    if not contractions:
-        raise ValueError("At least one `GeneralizedContractionShell` must be given.")
-    for c in contractions:
-        if not is_shell(c):
-            raise TypeError("Given contractions must be instances of the "
-                            "`GeneralizedContractionShell` class.")
-
-
 def _norm_types(coord_types, n):
     if not isinstance(coord_types, (list, tuple)):
         raise TypeError("`coord_types` must be a list or a tuple.")
@@ -59,8 +47,9 @@ def _norm_types(coord_types, n):
     return list(coord_types)
 
 
-class ElectronRepulsionIntegral:
-    """Electron-repulsion integrals of a basis, chemist notation (``(ab|cd)``)."""
+class ElectronRepulsionIntegral(BaseFourIndexSymmetric):
+    """Electron-repulsion integrals of a basis, chemist notation (``(ab|cd)``); a
+    ``BaseFourIndexSymmetric`` as in gbasis (``gbasis/integrals/electron_repulsion.py:20``)."""
 
     boys_func = staticmethod(_boys_host)
     _screen = 0.0
@@ -68,12 +57,8 @@ class ElectronRepulsionIntegral:
     _potential = (0, 0.0)  # two-electron operator (code, omega), see potential_code
 
     def __init__(self, contractions):
-        _check_contractions(contractions)
-        self._axes_contractions = (tuple(contractions),)
-
-    @property
-    def contractions(self):
-        return self._axes_contractions[0]
+        # argument checks and messages of gbasis/base.py:32-65
+        super().__init__(contractions)
 
     # ------------------------------------------------------------------ per quartet
     @classmethod
@@ -235,6 +220,10 @@ class ElectronRepulsionIntegralImproved(ElectronRepulsionIntegral):
     def construct_array_lincomb(self, transform, coord_type, device=None, **kwargs):
         return self._screened(kwargs, lambda: super(ElectronRepulsionIntegralImproved, self)
                               .construct_array_lincomb(transform, coord_type, device))
+
+
+# isinstance checks against gbasis's own base classes accept these (when gbasis is importable)
+register_with_gbasis(ElectronRepulsionIntegral, ElectronRepulsionIntegralImproved)
 
 
 def _lincomb_device(shells, types, transform, screen, device, potential=(0, 0.0)):

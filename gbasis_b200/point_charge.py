@@ -17,7 +17,7 @@ import ctypes
 import numpy as np
 
 from . import _engine
-from .electron_repulsion import _check_contractions
+from .base import check_shell_list
 
 __all__ = ["point_charge_integral", "nuclear_electron_attraction_integral"]
 
@@ -39,7 +39,7 @@ def _check_points(points_coords, points_charge):
 
 def _run(basis, points_coords, points_charge, sum_points, coord_type, device):
     import torch
-    _check_contractions(basis)
+    check_shell_list(basis)
     _check_points(points_coords, points_charge)
     types = None
     if coord_type is not None:

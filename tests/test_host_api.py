@@ -97,3 +97,62 @@ except ImportError:
         from gbasis_b200.synthetic import make_workload
         with pytest.raises(_engine.EngineError):
             er.electron_repulsion_integral(make_workload("tiny4"))
+
+
+def test_class_hierarchy_mirrors_gbasis():
+    """ElectronRepulsionIntegral is a BaseFourIndexSymmetric / BaseGaussianRelatedArray with the
+    reference's constructor contract (gbasis/base.py:32-65, gbasis/base_four_symm.py:70-93)."""
+    import pytest
+    from gbasis_b200.base import BaseGaussianRelatedArray
+    from gbasis_b200.base_four_symm import BaseFourIndexSymmetric
+    from gbasis_b200.electron_repulsion import (ElectronRepulsionIntegral,
+                                                ElectronRepulsionIntegralImproved)
+    from gbasis_b200.synthetic import make_workload
+    shells = make_workload("tiny4")
+    for cls in (ElectronRepulsionIntegral, ElectronRepulsionIntegralImproved):
+        obj = cls(shells)
+        assert isinstance(obj, BaseFourIndexSymmetric) and isinstance(obj, BaseGaussianRelatedArray)
+        assert obj.contractions == tuple(shells)
+        assert obj._axes_contractions == (tuple(shells),)
+    with pytest.raises(TypeError, match="list or tuple"):
+        ElectronRepulsionIntegral(shells[0])
+    with pytest.raises(ValueError, match="At least one"):
+        ElectronRepulsionIntegral([])
+    with pytest.raises(TypeError, match="must be instances"):
+        ElectronRepulsionIntegral([shells[0], 1.0])
+    with pytest.raises(TypeError):
+        BaseFourIndexSymmetric(shells)  # abstract, as in the reference
+
+
+def test_virtual_subclass_of_gbasis_base_classes():
+    """With gbasis importable, isinstance checks against its own base classes accept the
+    engine's objects (a stand-in gbasis package here: two ABCs)."""
+    import abc
+    import sys
+    import types
+    from gbasis_b200.base_four_symm import register_with_gbasis
+    from gbasis_b200.electron_repulsion import ElectronRepulsionIntegral
+    from gbasis_b200.synthetic import make_workload
+
+    class FakeBase(abc.ABC):
+        pass
+
+    class FakeFour(FakeBase):
+        pass
+    pkg = types.ModuleType("gbasis")
+    base = types.ModuleType("gbasis.base")
+    four = types.ModuleType("gbasis.base_four_symm")
+    base.BaseGaussianRelatedArray = FakeBase
+    four.BaseFourIndexSymmetric = FakeFour
+    saved = {k: sys.modules.get(k) for k in ("gbasis", "gbasis.base", "gbasis.base_four_symm")}
+    sys.modules.update({"gbasis": pkg, "gbasis.base": base, "gbasis.base_four_symm": four})
+    try:
+        assert register_with_gbasis(ElectronRepulsionIntegral)
+        obj = ElectronRepulsionIntegral(make_workload("tiny4"))
+        assert isinstance(obj, FakeFour) and isinstance(obj, FakeBase)
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                sys.modules.pop(k, None)
+            else:
+                sys.modules[k] = v
