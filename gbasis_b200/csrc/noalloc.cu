@@ -200,7 +200,7 @@ extern "C" int gbx_eri_full_noalloc(int n_shells, const int* angmom, const int* 
                           kPairClassL[h.ck][1], a, grid, st)))
       return s;
   }
-  ExpandArgs e;
+  ExpandArgs e{};  // zeroed: no fault word (this call's stores are never bounds-checked)
   e.n = B.nbf;
   e.nsh = n;
   e.notation = notation;
