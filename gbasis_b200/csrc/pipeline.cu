@@ -394,78 +394,6 @@ __device__ __forceinline__ void write_plane(const ExpandArgs& e, const double* _
   }
 }
 
-// The same plane written from its upper half.  A plane is symmetric (the ordered pairs (c, d)
-// and (d, c) have one pair function), so each table entry and staged value serves two
-// elements: rows are taken in quads c0..c0+3; for a column d beyond the quad, lane d reads
-// gtab[c0+i][d] (coalesced across the warp), stores the four values along the rows c0+i
-// (coalesced) and, as one 32-byte run, into row d at columns c0..c0+3 (two 16-byte streaming
-// stores when N is even and the planes 16-byte aligned, so that every run is; else four 8-byte
-// ones).  The
-// quads' own 4 x 4 diagonal blocks are written element by element.  Half the table loads and
-// shared-memory gathers of write_plane, a quarter fewer store instructions.
-template <bool PHYS>
-__device__ __forceinline__ void write_plane_sym(const ExpandArgs& e,
-                                                const double* __restrict__ s_row,
-                                                double* __restrict__ dst,
-                                                double* __restrict__ mir) {
-  const int* __restrict__ gtab = e.gtab;
-  const int n = (int)e.n;
-  const long long cs = PHYS ? (long long)n * n : (long long)n;  // row stride in the output
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int nq = (n + 3) >> 2;
-  // diagonal blocks: element (4k + i, 4k + j)
-  for (int t = threadIdx.x; t < nq * 16; t += blockDim.x) {
-    const int k = t >> 4, c = 4 * k + ((t >> 2) & 3), d = 4 * k + (t & 3);
-    if (c < n && d < n) {
-      const double v = s_row[__ldg(gtab + (long long)c * n + d)];
-      if (dst_ok(e, dst + c * cs + d)) __stcs(dst + c * cs + d, v);
-      if (mir && dst_ok(e, mir + c * cs + d)) __stcs(mir + c * cs + d, v);
-    }
-  }
-  // units (quad k, chunk of 32 columns beyond the quad's block), round robin over the warps;
-  // with N even every run starts at an even element offset from the plane's start, so 16-byte
-  // stores are aligned when the planes are
-  const bool vec = (n & 1) == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0 &&
-                   (reinterpret_cast<uintptr_t>(mir) & 15) == 0;
-  int k = 0, first = 0;  // quad of the warp's current unit and the units before that quad
-  for (int u = warp;; u += nw) {
-    int chunks = 0;
-    while (k < nq) {
-      chunks = (max(0, n - 4 * k - 4) + 31) >> 5;
-      if (u < first + chunks) break;
-      first += chunks;
-      ++k;
-    }
-    if (k >= nq) break;
-    const int c0 = 4 * k, d = c0 + 4 + 32 * (u - first) + lane;
-    if (d >= n) continue;
-    double v[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-      v[i] = c0 + i < n ? s_row[__ldg(gtab + (long long)(c0 + i) * n + d)] : 0.0;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      if (c0 + i >= n) break;
-      const long long at = (long long)(c0 + i) * cs + d;
-      if (dst_ok(e, dst + at)) __stcs(dst + at, v[i]);
-      if (mir && dst_ok(e, mir + at)) __stcs(mir + at, v[i]);
-    }
-    // row d, columns c0..c0+3 (c0 + 3 < n here, as d >= c0 + 4)
-    const long long at = (long long)d * cs + c0;
-    for (int pass = 0; pass < (mir ? 2 : 1); ++pass) {
-      double* __restrict__ p = (pass ? mir : dst) + at;
-      if (!dst_ok(e, p) || !dst_ok(e, p + 3)) continue;
-      if (vec) {
-        __stcs(reinterpret_cast<double2*>(p), make_double2(v[0], v[1]));
-        __stcs(reinterpret_cast<double2*>(p) + 1, make_double2(v[2], v[3]));
-      } else {
-#pragma unroll
-        for (int i = 0; i < 4; ++i) __stcs(p + i, v[i]);
-      }
-    }
-  }
-}
-
 __device__ __forceinline__ double* plane_ptr(const ExpandArgs& e, double* base, long long x,
                                              long long y, bool phys) {
   const long long n = e.n, n2 = n * n;
@@ -477,11 +405,11 @@ __device__ __forceinline__ void write_row_planes(const ExpandArgs& e, const doub
                                                  double* base, long long x, long long y,
                                                  bool mirror, bool phys) {
   if (phys)
-    write_plane_sym<true>(e, s_row, plane_ptr(e, base, x, y, true),
-                          mirror ? plane_ptr(e, base, y, x, true) : nullptr);
+    write_plane<true>(e, s_row, plane_ptr(e, base, x, y, true),
+                      mirror ? plane_ptr(e, base, y, x, true) : nullptr);
   else
-    write_plane_sym<false>(e, s_row, plane_ptr(e, base, x, y, false),
-                           mirror ? plane_ptr(e, base, y, x, false) : nullptr);
+    write_plane<false>(e, s_row, plane_ptr(e, base, x, y, false),
+                       mirror ? plane_ptr(e, base, y, x, false) : nullptr);
 }
 
 __global__ void __launch_bounds__(512) expand_rows(const ExpandArgs e) {
@@ -610,7 +538,7 @@ __global__ void gather_unique(const ExpandArgs e, const long long* __restrict__ 
 // Batch form of the row-staged expansion: molecule m's pair-function rows are the global rows
 // [row_first[m], row_first[m + 1]); each molecule has its own descriptor (tables, compact
 // store, output).
-__global__ void __launch_bounds__(512, 3) expand_rows_batch(const ExpandArgs* __restrict__ mols,
+__global__ void __launch_bounds__(512) expand_rows_batch(const ExpandArgs* __restrict__ mols,
                                                          const long long* __restrict__ row_first,
                                                          int nmol) {
   extern __shared__ double s_row[];
@@ -650,8 +578,8 @@ __global__ void __launch_bounds__(512) expand_slab(const ExpandArgs e, long long
     __syncthreads();
     stage_row(e, r, lr, s_row);
     __syncthreads();
-    if (phys) write_plane_sym<true>(e, s_row, plane_ptr(e, dst, x - x0, y, true), nullptr);
-    else write_plane_sym<false>(e, s_row, plane_ptr(e, dst, x - x0, y, false), nullptr);
+    if (phys) write_plane<true>(e, s_row, plane_ptr(e, dst, x - x0, y, true), nullptr);
+    else write_plane<false>(e, s_row, plane_ptr(e, dst, x - x0, y, false), nullptr);
   }
 }
 
@@ -1153,6 +1081,15 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
     GBX_CUDA(cudaEventRecord(B.fork, st), "fork");
     for (int j = 0; j < nstreams; ++j) GBX_CUDA(cudaStreamWaitEvent(B.aux[j], B.fork, 0), "fork wait");
   }
+  if (zero_list) {
+    // on the caller's stream, beside the class blocks (disjoint entries of the store)
+    const int zgrid = (int)std::max<long long>(
+        1, std::min<long long>((B.zero_cap + 7) / 8, (long long)nsm * 8));
+    zero_quartets<<<zgrid, 256, 0, st>>>(B.d_zero_work, B.d_zero_count, B.zero_cap, B.d_pairs,
+                                         B.d_shells, B.d_blocks, B.d_compact, B.compact_elems,
+                                         B.d_fault);
+    GBX_CUDA(cudaGetLastError(), "zero_quartets launch");
+  }
   for (int i = 0; i < nblk; ++i) {
     const int k = B.launch_order.empty() ? i : B.launch_order[i];
     const cudaStream_t bs = nstreams ? B.aux[i % nstreams] : st;
@@ -1200,16 +1137,6 @@ int run_compact(Basis& B, double tau, cudaStream_t st, double skip, double fp32)
       GBX_CUDA(cudaEventRecord(B.join[j], B.aux[j]), "join");
       GBX_CUDA(cudaStreamWaitEvent(st, B.join[j], 0), "join wait");
     }
-  }
-  if (zero_list) {
-    // after the class blocks, so that its CTAs take no SMs from the first class kernels; a
-    // small grid, as the list is short
-    const int zgrid = (int)std::max<long long>(
-        1, std::min<long long>((B.zero_cap + 7) / 8, (long long)nsm * 2));
-    zero_quartets<<<zgrid, 256, 0, st>>>(B.d_zero_work, B.d_zero_count, B.zero_cap, B.d_pairs,
-                                         B.d_shells, B.d_blocks, B.d_compact, B.compact_elems,
-                                         B.d_fault);
-    GBX_CUDA(cudaGetLastError(), "zero_quartets launch");
   }
   return GBX_OK;
 }
