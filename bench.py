@@ -466,7 +466,7 @@ def main():
                     help="which secondary configurations to measure (comma-separated)")
     ap.add_argument("--large64-atoms", type=int, default=16,
                     help="atoms of the 64-atom box in the direct-J configuration (64: the whole "
-                         "box, about 20 minutes on one B200)")
+                         "box: 6 minutes per J on one B200, FP64 and mixed)")
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
