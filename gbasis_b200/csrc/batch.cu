@@ -744,7 +744,7 @@ int gbx_batch_set_type_config(gbx_batch* b, int k, int variant, int ctas_per_sm)
   if (!b) return set_error(GBX_ERR_INVALID, "gbx_batch_set_type_config: null batch");
   Batch& B = *b->impl;
   if (k < 0 || k >= (int)B.types.size()) return set_error(GBX_ERR_INVALID, "type %d out of range", k);
-  if (variant < 0 || variant > 1) return set_error(GBX_ERR_INVALID, "variant must be 0 or 1");
+  if (variant < 0 || variant > 2) return set_error(GBX_ERR_INVALID, "variant must be 0, 1 or 2");
   if (ctas_per_sm < 1 || ctas_per_sm > 32)
     return set_error(GBX_ERR_INVALID, "ctas_per_sm must be in [1, 32]");
   BatchType& T = B.types[k];

@@ -32,7 +32,7 @@ constexpr long long kCoopMaxSmem = 227 * 1024;
 // staged programs: shared memory, not registers, is what limits these kernels' occupancy (a
 // class with f shells took 125 KB per 4-warp CTA with the largest chunks: 4 warps per SM).
 inline int coop_plan(const CoopMeta& M, long long phase_a, CoopArgs& A, size_t& smem, int& wpc,
-                     int max_warps_regs = 16, bool allow_staged = true) {
+                     int max_warps_regs = 16, bool allow_staged = true, int max_wpc = 4) {
   const int NCD = ncart(M.lc) * ncart(M.ld), NAB = ncart(M.la) * ncart(M.lb);
   const int NENF = M.NE * M.NF;
   const long long warp_cap = 48 * 1024 / 8;
@@ -55,7 +55,7 @@ inline int coop_plan(const CoopMeta& M, long long phase_a, CoopArgs& A, size_t& 
       for (int staged = 1; staged >= 0; --staged) {
         if (staged && (!allow_staged || prog_bytes > 32 * 1024)) continue;
         const long long prog = staged ? (prog_bytes + 15) / 16 * 16 : 0;
-        for (int w = 1; w <= 4; ++w) {
+        for (int w = 1; w <= max_wpc; ++w) {
           const long long cta = prog + extra + (long long)w * per_warp * 8;
           if (cta > kCoopMaxSmem) continue;
           const long long ctas = std::min<long long>(sm_bytes / (cta + reserved),
@@ -155,10 +155,27 @@ __device__ __forceinline__ void boys_lanes(int L, int lane, double T, double pre
   X[lane] = f * pref;
 }
 
-// Phases B-D of one quartet (bra pair pq.x, ket pair pq.y) from ACC = S[0 .. NE*NF).
-__device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv, double* S,
-                                          const int2 pq, const PairDev& P, const PairDev& Q,
-                                          const int lane) {
+// Threads that run one quartet's tail together: a warp (WarpGroup), or the NW warps of a CTA
+// that holds one quartet (CtaGroup<NW>).  t: the thread's index in the group; kN: its size;
+// sync(): the group's barrier.
+struct WarpGroup {
+  int t;
+  static constexpr int kN = 32;
+  __device__ __forceinline__ void sync() const { __syncwarp(); }
+};
+template <int NW>
+struct CtaGroup {
+  int t;
+  static constexpr int kN = 32 * NW;
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
+// Phases B-D of one quartet (bra pair pq.x, ket pair pq.y) from ACC = S[0 .. NE*NF), by the
+// threads of group g.  A group larger than a warp runs modes 0 (store) and 2 (Coulomb) only.
+template <class G>
+__device__ __forceinline__ void coop_tail_g(const CoopArgs& A, const ProgView& pv, double* S,
+                                            const int2 pq, const PairDev& P, const PairDev& Q,
+                                            const G& g) {
   const EriLaunch& a = A.a;
   const CoopMeta& M = A.m;
   auto INS = [&](int i) -> const short* { return pv.I(i); };
@@ -179,26 +196,26 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
   // HF[e][cd] overlays X (dead); rows are processed R at a time in KN
   for (int r0 = 0; r0 < M.NE; r0 += A.R) {
     const int rr = min(A.R, M.NE - r0);
-    for (int i = lane; i < rr * M.NF; i += 32) {
+    for (int i = g.t; i < rr * M.NF; i += G::kN) {
       const int r = i / M.NF, f = i - r * M.NF;
       KN[r * M.nK + f] = ACC[(r0 + r) * M.NF + f];
     }
-    __syncwarp();
+    g.sync();
     for (int l = 0; l < M.k_nlv; ++l) {
       const int b = kCoopLv[M.k_lv + l], e = kCoopLv[M.k_lv + l + 1], cnt = e - b;
-      for (int i = lane; i < rr * cnt; i += 32) {
+      for (int i = g.t; i < rr * cnt; i += G::kN) {
         const int r = i / cnt;
         const short* I = INS(M.k_ins + b + (i - r * cnt));
         double* Kr = KN + r * M.nK;
         Kr[I[0]] = fma(pick3(I[5], Q.ABx, Q.ABy, Q.ABz), Kr[I[2]], Kr[I[1]]);
       }
-      __syncwarp();
+      g.sync();
     }
-    for (int i = lane; i < rr * NCD; i += 32) {
+    for (int i = g.t; i < rr * NCD; i += G::kN) {
       const int r = i / NCD, j = i - r * NCD;
       HF[(r0 + r) * NCD + j] = KN[r * M.nK + IDX(M.kfin + j)];
     }
-    __syncwarp();
+    g.sync();
   }
   const ShellDev& sA = a.shells[P.shA];
   const ShellDev& sB = a.shells[P.shB];
@@ -210,20 +227,20 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
   const int nCi = schwarz ? NCC : n_int(sC), nDi = schwarz ? NCDD : n_int(sD);
   double mx = 0.0;
   if (coulomb) {
-    for (int i = lane; i < nAi * nBi; i += 32) {
+    for (int i = g.t; i < nAi * nBi; i += G::kN) {
       const int ua = i / nBi, ub = i - ua * nBi;
       VAB[i] = 0.0;
       DAB[i] = a.D[(sA.func_off + sA.pos[ua]) * a.nbf + sB.func_off + sB.pos[ub]] *
                sA.scl[ua] * sB.scl[ub];
     }
-    __syncwarp();
+    g.sync();
   }
   // ---------------------------------------------------------------- C
   if (nCi != NCC || nDi != NCDD) {
     for (int e = 0; e < M.NE; ++e) {
       double* row = HF + e * NCD;
       // axis D: T1[c][ud]
-      for (int i = lane; i < NCC * nDi; i += 32) {
+      for (int i = g.t; i < NCC * nDi; i += G::kN) {
         const int c = i / nDi, ud = i - c * nDi;
         double v;
         if (nDi != NCDD) {
@@ -235,9 +252,9 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
         }
         T1[i] = v;
       }
-      __syncwarp();
+      g.sync();
       // axis C: row[uc * nDi + ud]
-      for (int i = lane; i < nCi * nDi; i += 32) {
+      for (int i = g.t; i < nCi * nDi; i += G::kN) {
         const int uc = i / nDi, ud = i - uc * nDi;
         double v;
         if (nCi != NCC) {
@@ -249,7 +266,7 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
         }
         row[i] = v;
       }
-      __syncwarp();
+      g.sync();
     }
   }
   // ---------------------------------------------------------------- D
@@ -260,55 +277,55 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
   const bool tr = quartet_transposed(P, Q);  // values stored at [ket row][bra column]
   for (int c0 = 0; c0 < ncol; c0 += A.Cc) {
     const int cc = min(A.Cc, ncol - c0);
-    for (int i = lane; i < cc * M.NE; i += 32) {
+    for (int i = g.t; i < cc * M.NE; i += G::kN) {
       const int c = i / M.NE, e = i - c * M.NE;
       BN[c * M.nB + e] = HF[e * NCD + c0 + c];
     }
-    __syncwarp();
+    g.sync();
     for (int l = 0; l < M.b_nlv; ++l) {
       const int b = kCoopLv[M.b_lv + l], e = kCoopLv[M.b_lv + l + 1], cnt = e - b;
-      for (int i = lane; i < cc * cnt; i += 32) {
+      for (int i = g.t; i < cc * cnt; i += G::kN) {
         const int c = i / cnt;
         const short* I = INS(M.b_ins + b + (i - c * cnt));
         double* Bc = BN + c * M.nB;
         Bc[I[0]] = fma(pick3(I[5], P.ABx, P.ABy, P.ABz), Bc[I[2]], Bc[I[1]]);
       }
-      __syncwarp();
+      g.sync();
     }
-    for (int i = lane; i < cc * NAB; i += 32) {
+    for (int i = g.t; i < cc * NAB; i += G::kN) {
       const int c = i / NAB, j = i - c * NAB;
       OB[i] = BN[c * M.nB + IDX(M.bfin + j)];
     }
-    __syncwarp();
+    g.sync();
     // axis B then A (per column), result in OB as [c][ua][ub] with row stride nBi
     if (nBi != NCB) {
       const double* W = sph_mat(M.lb);
-      for (int i = lane; i < cc * NCA * nBi; i += 32) {
+      for (int i = g.t; i < cc * NCA * nBi; i += G::kN) {
         const int c = i / (NCA * nBi), rem = i - c * NCA * nBi, a_ = rem / nBi, ub = rem - a_ * nBi;
         double v = 0.0;
         for (int b = 0; b < NCB; ++b) v = fma(W[ub * NCB + b], OB[c * NAB + a_ * NCB + b], v);
         T2[c * NAB + a_ * nBi + ub] = v;
       }
     } else {
-      for (int i = lane; i < cc * NAB; i += 32) T2[i] = OB[i];
+      for (int i = g.t; i < cc * NAB; i += G::kN) T2[i] = OB[i];
     }
-    __syncwarp();
+    g.sync();
     if (nAi != NCA) {
       const double* W = sph_mat(M.la);
-      for (int i = lane; i < cc * nAi * nBi; i += 32) {
+      for (int i = g.t; i < cc * nAi * nBi; i += G::kN) {
         const int c = i / (nAi * nBi), rem = i - c * nAi * nBi, ua = rem / nBi, ub = rem - ua * nBi;
         double v = 0.0;
         for (int a_ = 0; a_ < NCA; ++a_) v = fma(W[ua * NCA + a_], T2[c * NAB + a_ * nBi + ub], v);
         OB[c * NAB + ua * nBi + ub] = v;
       }
     } else {
-      for (int i = lane; i < cc * NAB; i += 32) OB[i] = T2[i];
+      for (int i = g.t; i < cc * NAB; i += G::kN) OB[i] = T2[i];
     }
-    __syncwarp();
+    g.sync();
     if (coulomb) {
       // J[a][b] partial sums over this chunk's columns; J[c][d] of each column
       const int nab = nAi * nBi;
-      for (int i = lane; i < nab; i += 32) {
+      for (int i = g.t; i < nab; i += G::kN) {
         double s = VAB[i];
         for (int c = 0; c < cc; ++c) {
           const int col = c0 + c, uc = col / nDi, ud = col - uc * nDi;
@@ -319,7 +336,7 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
         VAB[i] = s;
       }
       if (pq.x != pq.y) {
-        for (int c = lane; c < cc; c += 32) {
+        for (int c = g.t; c < cc; c += G::kN) {
           const int col = c0 + c, uc = col / nDi, ud = col - uc * nDi;
           double s = 0.0;
           for (int i = 0; i < nab; ++i) s = fma(OB[c * NAB + i], DAB[i], s);
@@ -329,10 +346,10 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
           if (Q.shA != Q.shB) j_add(a, fd * a.nbf + fc, s);
         }
       }
-      __syncwarp();
+      g.sync();
       continue;
     }
-    for (int i = lane; i < cc * nAi * nBi; i += 32) {
+    for (int i = g.t; i < cc * nAi * nBi; i += G::kN) {
       const int c = i / (nAi * nBi), rem = i - c * nAi * nBi, ua = rem / nBi, ub = rem - ua * nBi;
       const int col = c0 + c, uc = col / nDi, ud = col - uc * nDi;
       if (schwarz) {
@@ -347,15 +364,17 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
       const long long rcd = (long long)Q.fo + sC.pos[uc] * nDo + sD.pos[ud];
       out_store(a, bbase + (tr ? rcd * bcols + rab : rab * bcols + rcd), v);
     }
-    __syncwarp();
+    g.sync();
   }
-  if (schwarz) {
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) a.qout[pq.x] = sqrt(mx);
+  if constexpr (G::kN == 32) {
+    if (schwarz) {
+      for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      if (g.t == 0) a.qout[pq.x] = sqrt(mx);
+    }
   }
   if (coulomb) {
     const double fk = (Q.shA != Q.shB) ? 2.0 : 1.0;
-    for (int i = lane; i < nAi * nBi; i += 32) {
+    for (int i = g.t; i < nAi * nBi; i += G::kN) {
       const int ua = i / nBi, ub = i - ua * nBi;
       const long long fa = sA.func_off + sA.pos[ua], fbn = sB.func_off + sB.pos[ub];
       const double s = VAB[i] * fk * sA.scl[ua] * sB.scl[ub];
@@ -363,7 +382,13 @@ __device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv,
       if (P.shA != P.shB) j_add(a, fbn * a.nbf + fa, s);
     }
   }
-  __syncwarp();
+  g.sync();
+}
+
+__device__ __forceinline__ void coop_tail(const CoopArgs& A, const ProgView& pv, double* S,
+                                          const int2 pq, const PairDev& P, const PairDev& Q,
+                                          const int lane) {
+  coop_tail_g(A, pv, S, pq, P, Q, WarpGroup{lane});
 }
 
 }  // namespace gbx

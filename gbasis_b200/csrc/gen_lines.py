@@ -296,12 +296,38 @@ def emit_class(S, tab_name, tab_off):
                     "s, W, ACC, first);")
     tag = _tag(S.cls)
     reg = tail_fits(S.cls)
+    # the group form (a CTA of GROUP_W warps per quartet, classes with the interpreted tail):
+    # vrr_xy on warp 0; each stage's rounds given to the warps longest first, each to the warp
+    # with the least work so far (a round's cost: its longest line); a CTA barrier between stages
+    body_g = []
+    if not reg:
+        stage = []
+
+        def flush():
+            load = [0] * GROUP_W
+            for cost, ln in sorted(stage, key=lambda x: -x[0]):
+                w = load.index(min(load))
+                load[w] += cost
+                body_g.append(f"    if (wq == {w})" + ln[3:])
+            stage.clear()
+        for ln in body:
+            if "__syncwarp();" in ln:
+                flush()
+                body_g.append("    __syncthreads();")
+            elif "lines_vrr_xy<" in ln:
+                body_g.append("    if (wq == 0)" + ln[3:])
+            else:
+                tmpl = ln[ln.index("<") + 1:ln.index(">")].split(",")
+                stage.append((int(tmpl[-1]) + 1 if "etr_z" not in ln else
+                              (int(tmpl[-2]) + 1) * (int(tmpl[-1]) + 1), ln))
+        flush()
     code = ([emit_tail(S.cls)] if reg else []) + [
             f"struct LinesCls_{tag} {{",
             f"  static constexpr int L = {L}, NE = {S.NE}, NF = {S.NF}, kW = {S.w_size}, "
             f"kY = {S.y_size};",
             f"  static constexpr int LA = {la}, LB = {lb}, LC = {lc}, LD = {ld};",
             f"  static constexpr bool kRegTail = {'true' if reg else 'false'};",
+            f"  static constexpr bool kGroup = {'false' if reg else 'true'};",
             f"  using Tail = {'TailCls_' + tag if reg else 'void'};",
             "  static __device__ __forceinline__ void prim(int lane, const double* Fs,",
             "                                              const LinePS& s, double* __restrict__ W,",
@@ -309,6 +335,13 @@ def emit_class(S, tab_name, tab_off):
             "                                              double* __restrict__ ACC, bool first) {",
             *body,
             "  }",
+            *([] if reg else [
+                "  static __device__ __forceinline__ void prim_g(int wq, int lane, const double* Fs,",
+                "                                                const LinePS& s, double* __restrict__ W,",
+                "                                                double* __restrict__ Y,",
+                "                                                double* __restrict__ ACC, bool first) {",
+                *body_g,
+                "  }"]),
             "};"]
     return "\n".join(code), tab
 
@@ -430,6 +463,7 @@ def emit_tail(cls):
 
 
 # ------------------------------------------------------------------- split register kernel
+GROUP_W = 4         # warps of the group form's CTA (one quartet per CTA)
 SPLITS = (4, 8)     # warps of a CTA, each computing one part of the targets
 SPLIT_MAX_ACC = 64  # accumulators per thread in a part
 SPLIT_MAX_OPS = 500  # recursion operations per part with 4 parts

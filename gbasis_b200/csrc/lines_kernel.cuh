@@ -26,6 +26,9 @@ namespace gbx {
 
 __host__ __device__ constexpr int lines_tet(int k) { return k * (k + 1) * (k + 2) / 6; }
 
+// Warps per CTA of the line kernel's group form (gen_lines.py GROUP_W).
+constexpr int kLinesGroupW = 4;
+
 // Offset of (ex, ey, 0) in a tetrahedral block of extent g (ex + ey + ez <= g).
 __host__ __device__ constexpr int lines_toff(int ex, int ey, int g) {
   return lines_tet(g + 1) - lines_tet(g + 1 - ex) + ey * (g + 1 - ex) - ey * (ey - 1) / 2;
@@ -419,6 +422,90 @@ __global__ void __launch_bounds__(128, 4) eri_lines(const CoopArgs A) {
   }
 }
 
+// Group form of the line kernel, for classes with the interpreted tail whose per-warp buffers
+// leave few warps on an SM: a CTA of kLinesGroupW warps holds one quartet in one buffer.  Per
+// primitive quartet warp 0 evaluates the Boys values, then C::prim_g runs each stage's rounds of
+// lines on the warps the generator gave them (vrr_xy on warp 0), with a CTA barrier between
+// stages; the interpreted tail then runs on all the CTA's threads (modes 0 and 2).  Same
+// arithmetic per line and per tail step as eri_lines.
+template <class C>
+__global__ void __launch_bounds__(32 * kLinesGroupW, 4) eri_lines_grp(const CoopArgs A) {
+  extern __shared__ double smem[];
+  const EriLaunch& a = A.a;
+  const CoopMeta& M = A.m;
+  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+  const long long count = a.work_count ? (long long)(*a.work_count) : a.nwork;
+  if ((long long)blockIdx.x >= count) return;  // no quartet for this CTA (uniform)
+  short(*s_ins)[8] = reinterpret_cast<short(*)[8]>(smem);
+  short* s_idx = reinterpret_cast<short*>(smem) + 8 * M.n_ins;
+  const bool staged = A.prog_doubles > 0;
+  if (staged) {
+    const int4* src = reinterpret_cast<const int4*>(&kCoopIns[M.v_ins][0]);
+    int4* dst4 = reinterpret_cast<int4*>(smem);
+    for (int i = threadIdx.x; i < M.n_ins; i += blockDim.x) dst4[i] = src[i];
+    for (int i = threadIdx.x; i < M.n_idx; i += blockDim.x) s_idx[i] = kCoopIdx[M.targets + i];
+  }
+  const ProgView pv = staged ? ProgView{s_ins, s_idx, M.v_ins, M.targets}
+                             : ProgView{kCoopIns, kCoopIdx, 0, 0};
+  double* S = smem + A.prog_doubles;
+  double* ACC = S;
+  double* W = S + C::NE * C::NF;
+  double* Y = W + C::kW;
+  double* Fs = Y + C::kY;
+  unsigned long long* const tk = a.ticket;  // one quartet per draw, by thread 0
+  __shared__ long long s_w;
+  long long w = blockIdx.x;
+  for (;;) {
+    if (tk) {
+      if (threadIdx.x == 0) s_w = (long long)atomicAdd(tk, 1ull);
+      __syncthreads();  // also: programs staged (first quartet), previous tail done
+      w = s_w;
+    } else {
+      __syncthreads();
+    }
+    if (w >= count) break;  // the same for all threads of the CTA
+    const int2 pq = a.work[a.reverse ? a.work_off + a.nwork - 1 - w : a.work_off + w];
+    const PairDev P = a.pairs[pq.x];
+    const PairDev Q = a.pairs[pq.y];
+    const int np = P.nprim * Q.nprim;
+    for (int idx = 0; idx < np; ++idx) {
+      const int ip = idx / Q.nprim, jq = idx - ip * Q.nprim;
+      const PrimPair bp = a.prims[P.prim_off + ip], kp = a.prims[Q.prim_off + jq];
+      const double r = rsqrt(bp.zeta + kp.zeta);
+      const double inv = r * r;
+      const double PQx = bp.Px - kp.Px, PQy = bp.Py - kp.Py, PQz = bp.Pz - kp.Pz;
+      const double rz = kp.zeta * inv;
+      const double T = bp.zeta * rz * fma(PQx, PQx, fma(PQy, PQy, PQz * PQz));
+      LinePS ps;
+      ps.PAx = bp.Xx;
+      ps.PAy = bp.Xy;
+      ps.PAz = bp.Xz;
+      ps.WPx = -rz * PQx;
+      ps.WPy = -rz * PQy;
+      ps.WPz = -rz * PQz;
+      ps.o2z = 0.5 * bp.izeta;
+      ps.rz = rz;
+      ps.ze = bp.zeta * kp.izeta;
+      ps.o2e = 0.5 * kp.izeta;
+      ps.CEx = fma(ps.ze, bp.Xx, kp.Xx);
+      ps.CEy = fma(ps.ze, bp.Xy, kp.Xy);
+      ps.CEz = fma(ps.ze, bp.Xz, kp.Xz);
+      if (wq == 0)
+        boys_lanes(C::L, lane, T, bp.C * kp.C * r, a.boys_tab, Fs, a.potential, a.omega,
+                   bp.zeta * rz);
+      __syncthreads();
+      C::prim_g(wq, lane, Fs, ps, W, Y, ACC, idx == 0);
+      __syncthreads();
+    }
+    if (np == 0) {  // no primitive quartet (a pair left without primitives): zero targets
+      for (int i = threadIdx.x; i < C::NE * C::NF; i += blockDim.x) ACC[i] = 0.0;
+      __syncthreads();
+    }
+    coop_tail_g(A, pv, S, pq, P, Q, CtaGroup<kLinesGroupW>{(int)threadIdx.x});
+    if (!tk) w += gridDim.x;
+  }
+}
+
 // Launch of the line kernel of class C (same shared-memory plan as the interpreted kernel,
 // with phase A's W, Y and Boys buffers).
 template <class C>
@@ -445,6 +532,38 @@ int launch_lines_t(const EriLaunch& a, const CoopMeta& m, cudaStream_t st) {
     s = coop_plan(m, (long long)C::kW + C::kY + C::L + 1, A, smem, wpc);
   }
   if (s) return s;
+  if constexpr (C::kGroup) {
+    // group form (a.variant 2), or by default (a.variant 0) for classes whose ket pair has no
+    // s shell first (LC >= 1); not for the Schwarz diagonal (mode 1).  Measured per class on the
+    // 20-atom chain's unique integrals, blocks one after another: the group form took up to
+    // 55 % off the classes with LC >= 1 ((ff|df) 107 -> 56 ms, (ff|ff) 54 -> 25, (ff|pf)
+    // 84 -> 65; three within 5 % either way) and cost up to 100 % on most LC = 0 classes
+    // ((df|sp) 77 -> 156 ms)
+    CoopArgs G;
+    G.a = a;
+    G.m = m;
+    size_t gsmem = 0;
+    int one = 1;
+    // the kernel's own 8-byte ticket slot sits in static shared memory beside the plan's
+    const bool group = a.mode != 1 &&
+                       (a.variant == 2 || (a.variant == 0 && C::LC >= 1)) &&
+                       coop_plan(m, (long long)C::kW + C::kY + C::L + 1, G, gsmem, one,
+                                 16 / kLinesGroupW, true, 1) == GBX_OK &&
+                       (long long)gsmem + 64 <= kCoopMaxSmem;
+    if (group) {
+      s = cuda_status(cudaFuncSetAttribute(eri_lines_grp<C>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)gsmem), "eri_lines_grp shared memory attribute");
+      if (s) return s;
+      int dev = 0, nsm = 1;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      const long long grid = std::max<long long>(
+          1, std::min<long long>(a.nwork, (long long)nsm * (16 / kLinesGroupW)));
+      eri_lines_grp<C><<<(int)grid, 32 * kLinesGroupW, gsmem, st>>>(G);
+      return cuda_status(cudaGetLastError(), "eri_lines_grp launch");
+    }
+  }
   // the Coulomb epilogue (mode 2) is a separate instantiation, so that the store / Schwarz
   // kernel of a class with the register tail carries no interpreted tail
   auto kern = a.potential ? (a.mode == 2 ? eri_lines<C, true, true> : eri_lines<C, false, true>)

@@ -737,7 +737,7 @@ int gbx_set_block_config(gbx_basis* b, int k, int variant, int ctas_per_sm) {
   if (!b) return set_error(GBX_ERR_INVALID, "gbx_set_block_config: null basis");
   Basis& B = *b->impl;
   if (k < 0 || k >= (int)B.blocks.size()) return set_error(GBX_ERR_INVALID, "block %d out of range", k);
-  if (variant < 0 || variant > 1) return set_error(GBX_ERR_INVALID, "variant must be 0 or 1");
+  if (variant < 0 || variant > 2) return set_error(GBX_ERR_INVALID, "variant must be 0, 1 or 2");
   if (ctas_per_sm < 1 || ctas_per_sm > 32)
     return set_error(GBX_ERR_INVALID, "ctas_per_sm must be in [1, 32]");
   B.blocks[k].variant = variant;

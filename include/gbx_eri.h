@@ -262,8 +262,11 @@ int gbx_block_info(const gbx_basis* b, int k, int* cls4, int* team, double* avg_
                    int64_t* n_quartets);
 int gbx_set_team(gbx_basis* b, int k, int team);
 /* Further launch knobs of block k (the autotuner's): variant 0 runs a heavy class that has
- * both kernels on the split register kernel, 1 on the line kernel (no effect on other
- * classes); ctas_per_sm (1..32) caps the register kernel's grid at that many CTAs per SM.
+ * both kernels on the split register kernel, 1 on the line kernel; for the classes whose line
+ * kernel has the interpreted tail, 0 picks between the one-warp-per-quartet line kernel and
+ * its group form (a CTA of 4 warps per quartet) by the warps the former keeps resident, 1
+ * forces the former and 2 the group form (no effect on other classes); ctas_per_sm (1..32)
+ * caps the register kernel's grid at that many CTAs per SM.
  * gbx_basis_set_streams: number of concurrent streams (1..16, default 6) the class blocks of
  * a call are spread over.  No reference counterpart (gbasis runs one quartet at a time). */
 int gbx_set_block_config(gbx_basis* b, int k, int variant, int ctas_per_sm);
