@@ -315,3 +315,46 @@ def test_split_parts_cover_targets(cls):
     Ed = direct(cls, s, Fs)
     ref = np.array([Ed(e, f) for e in E for f in F])
     np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())
+
+
+def _stages(lines):
+    """Split generated prim code into stages at the barriers: per stage the round calls."""
+    out, cur = [], []
+    for ln in lines:
+        if "__syncwarp();" in ln or "__syncthreads();" in ln:
+            out.append(cur)
+            cur = []
+        elif "lines_" in ln:
+            cur.append(ln)
+    out.append(cur)
+    return out
+
+
+def test_group_form_runs_every_round_once():
+    """The line kernel's group form (prim_g, a CTA of GROUP_W warps per quartet) runs exactly
+    the one-warp prim's calls, stage by stage, each on one warp in range (vrr_xy on warp 0)."""
+    heavy = [c for c in gen_eri.canonical_classes(3) if not gen_eri.is_light(c)]
+    grouped = 0
+    for c in heavy:
+        code, _ = gen_lines.emit_class(gen_lines.Schedule(*c), "kLinesTab", 0)
+        has = "prim_g(" in code
+        assert has == (not gen_lines.tail_fits(c)), c
+        if not has:
+            continue
+        grouped += 1
+        one = code[code.index("void prim("):code.index("prim_g(")].splitlines()
+        grp = code[code.index("prim_g("):].splitlines()
+        s1, s2 = _stages(one), _stages(grp)
+        assert len(s1) == len(s2), c
+        for a, b in zip(s1, s2):
+            calls = []
+            for ln in b:
+                m = re.match(r"\s*if \(wq == (\d+)\) (lines_.*)$", ln)
+                assert m, (c, ln)
+                w = int(m.group(1))
+                assert 0 <= w < gen_lines.GROUP_W
+                if "lines_vrr_xy<" in ln:
+                    assert w == 0
+                calls.append(m.group(2).strip())
+            assert sorted(x.strip() for x in a) == sorted(calls), c
+    assert grouped > 0
